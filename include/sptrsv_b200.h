@@ -1,0 +1,284 @@
+/*
+ * sptrsv_b200.h — C ABI of the B200-native sparse lower-triangular solver.
+ *
+ * Drop-in boundary for the CSR SpTRSV path of HCL-Fing/SPTRSV.  The first
+ * block keeps the reference's types and entry points with the same names,
+ * struct layouts, MODE values and parameter orders, wrapped in extern "C" so
+ * that a reference caller recompiles unchanged and any FFI (ctypes, cgo, JNI)
+ * can bind the symbols by name.  The second block adds new symbols only; no
+ * reference symbol changes meaning.
+ *
+ * Matrix convention (as in the reference): square lower-triangular CSR,
+ * 0-based, int32 indices, columns strictly increasing inside a row and the
+ * diagonal stored LAST in every row (the reference kernels read
+ * val[rowptr[i+1]-1] as the diagonal, solver/solve_csr_simple.cu:45).
+ *
+ * VALUE_TYPE is fixed to double, the reference's default
+ * (Makefile:7, header/common.h:28).  FP32 work happens inside the library.
+ *
+ * Error behaviour: functions that return int in the reference return 0 on
+ * success and a negative SPTRSV_ERR_* code on failure (the reference only
+ * printed, header/common.h:163-168).  Functions that return void in the
+ * reference record their outcome in a thread-local last error, read with
+ * sptrsv_last_error() / sptrsv_last_error_string().  No device wait in this
+ * library is unbounded: a wait that runs out sets a device status word and
+ * returns, and the host reports SPTRSV_ERR_TIMEOUT.
+ */
+#ifndef SPTRSV_B200_H
+#define SPTRSV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifndef VALUE_TYPE
+#define VALUE_TYPE double
+#endif
+
+/* Same typedef as CUDA's driver_types.h, so both headers can be included. */
+struct CUstream_st;
+typedef struct CUstream_st* cudaStream_t;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Reference types (header/dfr_syncfree.h:7-41), same layout and values.      */
+/* ------------------------------------------------------------------------- */
+
+/* header/dfr_syncfree.h:7-12 */
+typedef enum MODE { SIMPLE = 0, ORDER = 1, MULTIROW = 2, ALL = 3 } MODE;
+
+/* header/dfr_syncfree.h:14-23 — device CSR handle.  ia[nr+1], ja[nnz],
+ * a[nnz] are device pointers owned by the library after allocate_memory. */
+typedef struct {
+    int nr;
+    int nc;
+    int nnz;
+    int* ia;
+    int* ja;
+    VALUE_TYPE* a;
+} sp_mat_t;
+
+/* header/dfr_syncfree.h:25-41 — analysis result.  All pointers are device
+ * arrays owned by the library and released by free_device_analysis.
+ *   iorder[nr]            rows stably sorted by key 7*(level-1)+bucket
+ *   ibase_row[n_warps+1]  first iorder position of each multirow warp
+ *   ivect_size_warp[n_warps] lanes per row of each multirow warp (0: diagonal-only rows)
+ *   row_ctr[1]            ticket / status word
+ * Fields the reference declares but never fills are filled here:
+ *   lev_size[nlevs]       rows per level
+ *   warp_lev[n_warps]     level (1-based) of each multirow warp
+ *   inv_iorder[nr]        position of each row in iorder
+ *   lev_ctr               0 */
+typedef struct {
+    MODE mode;
+    int lev_ctr;
+    int nlevs;
+    int* lev_size;
+    int* warp_lev;
+    int n_warps;
+    int* inv_iorder;
+    int* iorder;
+    int* ibase_row;
+    int* ivect_size_warp;
+    int* row_ctr;
+} dfr_analysis_info_t;
+
+/* ------------------------------------------------------------------------- */
+/* Reference entry points.                                                    */
+/* ------------------------------------------------------------------------- */
+
+/* Replaces header/interface.h:6 (defined at interface.cu:9).  Copies a host
+ * CSR (n rows, nnz = csrRowPtrL[n]-csrRowPtrL[0]) to the device and fills the
+ * caller-allocated *gpu_L.  `mode` is recorded for run_analysis callers that
+ * do not set info->mode themselves.  Returns 0, or a negative code when the
+ * CSR is not lower triangular with the diagonal last. */
+int allocate_memory(int* csrRowPtrL, int* csrColIdxL, VALUE_TYPE* csrValL, int n,
+                    sp_mat_t* gpu_L, MODE mode);
+
+/* Replaces header/interface.h:7 (defined at interface.cu:28).  Reads
+ * info->mode; returns -1 for SIMPLE (no analysis needed, interface.cu:29),
+ * 0 after filling *info, or a negative SPTRSV_ERR_* code. */
+int run_analysis(dfr_analysis_info_t* info, sp_mat_t* gpu_L);
+
+/* Replaces header/interface.h:8 (defined at interface.cu:40).  b and x are
+ * HOST arrays of n values; x receives the solution of L x = b.  Dispatch as
+ * in interface.cu:68-90: SIMPLE when info is NULL, else by info->mode
+ * (ORDER, MULTIROW; ALL runs MULTIROW).  Outcome in sptrsv_last_error(). */
+void run_solver(sp_mat_t* gpu_L, dfr_analysis_info_t* info, VALUE_TYPE* b, VALUE_TYPE* x, int n);
+
+/* Replaces header/interface.h:9 (defined at interface.cu:97).  Frees every
+ * device array of *gpu_L and *info and zeroes the pointers.  The structs
+ * themselves stay caller-owned.  Either argument may be NULL. */
+void free_device_analysis(sp_mat_t* gpu_L, dfr_analysis_info_t* info);
+
+/* Replaces header/analysis.h:20 (defined at analysis/analysis_csr.cu:272).
+ * *info must point to a caller-allocated struct.  Computes levels, nlevs,
+ * iorder and, for MULTIROW/ALL, the multirow warp map, bit-exact with the
+ * reference.  Outcome in sptrsv_last_error(). */
+void multirow_analysis_base_GPU(dfr_analysis_info_t** info, sp_mat_t* gpu_L, MODE mode);
+
+/* Replaces header/solver.h:5 (solver/solve_csr_simple.cu:141).  Sync-free
+ * solve in natural row order, no analysis.  b, x are DEVICE arrays.
+ * is_solved is accepted for signature compatibility and may be NULL: the
+ * kernel uses x itself as the readiness flag.  Runs on the legacy default
+ * stream like the reference.  Outcome in sptrsv_last_error() (launch errors
+ * only; call sptrsv_sync_status for device-side errors). */
+void csr_L_solve_simple(sp_mat_t* mat, const VALUE_TYPE* b, VALUE_TYPE* x, int n, int* is_solved);
+
+/* Replaces header/solver.h:6 (solver/solve_csr_order.cu:171).  Rows in
+ * iorder sequence, one warp per row.  b, x are DEVICE arrays; stream-ordered. */
+void csr_L_solve_order(sp_mat_t* mat, dfr_analysis_info_t* info, const VALUE_TYPE* b,
+                       VALUE_TYPE* x, int n, cudaStream_t stream);
+
+/* Replaces header/solver.h:7 (solver/solve_csr_multirow.cu:116).  1-32 rows
+ * per warp from the analysis warp map.  b, x are DEVICE arrays. */
+void csr_L_solve_multirow(sp_mat_t* mat, dfr_analysis_info_t* info, const VALUE_TYPE* b,
+                          VALUE_TYPE* x, int n, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Extensions (new symbols; no counterpart changes meaning).                  */
+/* ------------------------------------------------------------------------- */
+
+#define SPTRSV_OK                 0
+#define SPTRSV_NO_ANALYSIS       -1  /* run_analysis on SIMPLE (interface.cu:29) */
+#define SPTRSV_ERR_INVALID_ARG   -2
+#define SPTRSV_ERR_INVALID_CSR   -3
+#define SPTRSV_ERR_CUDA          -4
+#define SPTRSV_ERR_TIMEOUT       -5
+#define SPTRSV_ERR_NOT_ANALYSED  -6
+#define SPTRSV_ERR_ALLOC         -7
+#define SPTRSV_ERR_NOT_CONVERGED -8
+#define SPTRSV_ERR_UNSUPPORTED   -9
+
+/* Thread-local outcome of the last call on this host thread. */
+int sptrsv_last_error(void);
+const char* sptrsv_last_error_string(void);
+const char* sptrsv_version(void);
+
+/* Waits for `stream`, then reads and clears the device status word that the
+ * kernels of this library set when a bounded wait runs out.  Returns 0 or
+ * SPTRSV_ERR_TIMEOUT / SPTRSV_ERR_CUDA. */
+int sptrsv_sync_status(cudaStream_t stream);
+
+/* Device-wait budget of every bounded spin in nanoseconds (default 2 s).
+ * A wait that exceeds it aborts the kernel with SPTRSV_ERR_TIMEOUT. */
+void sptrsv_set_wait_budget_ns(unsigned long long ns);
+
+/* Failure-path self test: one device thread waits on a word that nothing
+ * ever writes.  Returns SPTRSV_ERR_TIMEOUT once the bounded wait gives up
+ * (after budget_ns); the context stays usable. */
+int sptrsv_selftest_bounded_wait(unsigned long long budget_ns);
+
+/* Checks that a HOST CSR is lower triangular with sorted columns and the
+ * diagonal last.  Returns 0 or SPTRSV_ERR_INVALID_CSR; *bad_row gets the
+ * first offending row (or -1).  Pure host code. */
+int sptrsv_check_csr_host(const int* rowptr, const int* colidx, int n, int* bad_row);
+
+/* Copies the 1-based level of every row (the reference's intermediate
+ * dfr_analysis_info array, analysis_csr.cu:181) into host_levels[nr]. */
+int sptrsv_analysis_levels(const dfr_analysis_info_t* info, int* host_levels);
+
+/* Copies the per-key row counts buckets[7*nlevs] (analysis_csr.cu:336-348)
+ * into host_buckets. */
+int sptrsv_analysis_buckets(const dfr_analysis_info_t* info, int* host_buckets);
+
+/* Order-coop variant (solver/solve_csr_order.cu:11-77, disabled in the
+ * reference by ORDER_COOP 0): iorder sequence, `tile` lanes per row
+ * (tile in {1,2,4,8,16,32}).  b, x DEVICE arrays. */
+int sptrsv_solve_order_tile(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b,
+                            double* x, int tile, cudaStream_t stream);
+
+/* --- Solve plans: the optimised path ------------------------------------- */
+/* A plan owns a solve-optimised copy of the matrix built from (gpu_L, info):
+ * rows stored in level order, inverse diagonal split out, an FP32 copy of
+ * the values, and the chosen schedule.  It does not alias gpu_L->a: after a
+ * value change call sptrsv_plan_update_values. */
+typedef struct sptrsv_plan_s* sptrsv_plan_t;
+
+/* Solve variants a schedule can pick. */
+#define SPTRSV_VAR_SIMPLE    0  /* natural row order, no analysis needed      */
+#define SPTRSV_VAR_ORDER     1  /* level order, fixed lanes per row           */
+#define SPTRSV_VAR_MULTIROW  2  /* level order, lanes per row by row length    */
+#define SPTRSV_VAR_CLUSTER   3  /* level order, block-local readiness in smem  */
+#define SPTRSV_N_VARIANTS    4
+
+typedef struct {
+    int variant;          /* SPTRSV_VAR_*                                      */
+    int rows_per_warp;    /* 1,2,4,8,16,32 (lanes per row = 32/rows_per_warp;  */
+                          /* for MULTIROW it caps the rows packed per warp)    */
+    int block_warps;      /* warps per CTA (1..32)                             */
+    int ir_max_iters;     /* FP32+IR: refinement steps after the first solve   */
+} sptrsv_schedule_t;
+
+/* Creates a plan for the analysed matrix.  info must come from run_analysis
+ * or multirow_analysis_base_GPU on gpu_L (any mode but SIMPLE). */
+int sptrsv_plan_create(const sp_mat_t* gpu_L, const dfr_analysis_info_t* info, sptrsv_plan_t* plan);
+int sptrsv_plan_destroy(sptrsv_plan_t plan);
+int sptrsv_plan_set_schedule(sptrsv_plan_t plan, const sptrsv_schedule_t* s);
+int sptrsv_plan_get_schedule(sptrsv_plan_t plan, sptrsv_schedule_t* s);
+/* Re-reads gpu_L->a (same pattern) into the plan's value copies. */
+int sptrsv_plan_update_values(sptrsv_plan_t plan, const sp_mat_t* gpu_L);
+
+/* Plain FP64 solve of L X = B for nrhs right-hand sides (1..32).  B and X
+ * are DEVICE arrays, row-major n x nrhs (value (i,k) at i*nrhs+k). */
+int sptrsv_solve_f64(sptrsv_plan_t plan, const double* b, double* x, int nrhs, cudaStream_t stream);
+
+/* FP32 solve with FP64 iterative refinement: x0 = solve32(b); then
+ * ir_max_iters times r = b - L x (FP64), d = solve32(r), x += d (FP64).
+ * Same layout as sptrsv_solve_f64. */
+int sptrsv_solve_ir(sptrsv_plan_t plan, const double* b, double* x, int nrhs, cudaStream_t stream);
+
+/* The inner FP32 solve of sptrsv_solve_ir on its own: x32 (DEVICE, n x nrhs
+ * floats) = L^-1 b with FP32 values and accumulation, b read as FP64. */
+int sptrsv_solve_f32(sptrsv_plan_t plan, const double* b, float* x32, int nrhs, cudaStream_t stream);
+
+/* Host-buffer convenience of sptrsv_solve_ir / sptrsv_solve_f64 (copies in
+ * and out on `stream` through plan-owned device buffers; precision 32 picks
+ * FP32+IR, 64 plain FP64). */
+int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, int nrhs,
+                      int precision, cudaStream_t stream);
+
+/* FP64 residual r = b - L x on the device (row-major n x nrhs). */
+int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, double* r,
+                        int nrhs, cudaStream_t stream);
+
+/* --- Synthetic inputs (host code) ---------------------------------------- */
+/* The reference reads SuiteSparse .mtx files (main.cu:66-246); none ship with
+ * it.  These seeded generators make the benchmark matrices: square
+ * lower-triangular CSR, sorted columns, diagonal last.  Arrays are malloc'd;
+ * release them with sptrsv_host_csr_free. */
+typedef struct {
+    int n;
+    int nnz;
+    int* rowptr;
+    int* colidx;
+    double* val;
+} sptrsv_host_csr_t;
+
+/* Row i: k ~ U{off_min..off_max} (capped by the window) distinct columns
+ * uniform in [max(0,i-bandwidth), i-1]; off-diagonals U(-1,1), diagonal
+ * 1 + sum|offdiag|. */
+int sptrsv_gen_banded(int n, int bandwidth, int off_min, int off_max, uint64_t seed, sptrsv_host_csr_t* out);
+/* Strict lower triangle plus diagonal of the 5-point Laplacian on an nx x ny
+ * grid (row-major): neighbours -1 + U(-0.1,0.1), diagonal 4. */
+int sptrsv_gen_grid2d(int nx, int ny, uint64_t seed, sptrsv_host_csr_t* out);
+/* Same for the 7-point Laplacian on nx x ny x nz, diagonal 6. */
+int sptrsv_gen_grid3d(int nx, int ny, int nz, uint64_t seed, sptrsv_host_csr_t* out);
+/* Off-diagonal count min(Z-1, max_off, i), Z ~ Zipf(s) on {1,2,...};
+ * columns distinct, uniform over all preceding rows; diagonally dominant. */
+int sptrsv_gen_zipf(int n, double s, int max_off, uint64_t seed, sptrsv_host_csr_t* out);
+/* Block diagonal with dense lower-triangular blocks; diagonally dominant. */
+int sptrsv_gen_blockdiag(int n, int block, uint64_t seed, sptrsv_host_csr_t* out);
+void sptrsv_host_csr_free(sptrsv_host_csr_t* m);
+/* dist 0: ones, 1: U(-1,1), 2: N(0,1). */
+int sptrsv_gen_vector(long long m, int dist, uint64_t seed, double* out);
+/* y = L x on the host, row-major nrhs. */
+int sptrsv_host_spmv(const sptrsv_host_csr_t* m, const double* x, double* y, int nrhs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPTRSV_B200_H */

@@ -1,0 +1,124 @@
+// common.cuh — device helpers shared by the analysis and solve kernels.
+//
+// Readiness protocol (the reference's NaN-sentinel scheme,
+// solver/solve_csr_order.cu:180 and :258-260, with explicit memory order):
+// before a solve the output vector is filled with all-ones bits; a row's
+// value is its own readiness flag.  Writers store the finished value with a
+// relaxed gpu-scope store, readers poll with relaxed gpu-scope loads (L2,
+// no L1 allocation).  The value is the only datum passed, and a naturally
+// aligned 32/64-bit access is single-copy atomic, so relaxed order suffices
+// and no fence sits on the dependency path.  A computed value whose bits
+// equal the sentinel (a negative NaN with all mantissa bits set) is replaced
+// by the canonical quiet NaN so that readers never wait on a finished row.
+//
+// Every wait is bounded: it polls a device status word and a %globaltimer
+// deadline; on expiry it records SPTRSV_ERR_TIMEOUT and the row, and every
+// other waiting warp leaves at its next poll of the status word.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sptrsv_b200.h"
+
+namespace sptrsv {
+
+constexpr int kWarp = 32;
+
+// Device status block: [0] error code (0 = ok), [1] first offending row.
+struct DevStatus {
+    int code;
+    int row;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ double ld_relaxed(const double* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ float ld_relaxed(const float* p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return __uint_as_float(v);
+}
+__device__ __forceinline__ int ld_relaxed(const int* p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v))
+                 : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(__float_as_uint(v)) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(int* p, int v)
+{
+    asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Sentinel tests: the fill pattern is all-ones bits (memset 0xFF).  For
+// doubles the reference tests the high word only (solve_csr_order.cu:260).
+__device__ __forceinline__ bool is_pending(double v) { return __double2hiint(v) == (int)0xFFFFFFFF; }
+__device__ __forceinline__ bool is_pending(float v) { return __float_as_uint(v) == 0xFFFFFFFFu; }
+// Levels are >= 1 once written; the level array is zero-filled.
+__device__ __forceinline__ bool is_pending(int v) { return v == 0; }
+
+__device__ __forceinline__ double publishable(double v)
+{
+    return __double2hiint(v) == (int)0xFFFFFFFF ? __longlong_as_double(0x7FF8000000000000LL) : v;
+}
+__device__ __forceinline__ float publishable(float v)
+{
+    return __float_as_uint(v) == 0xFFFFFFFFu ? __uint_as_float(0x7FC00000u) : v;
+}
+
+__device__ __forceinline__ void report(DevStatus* st, int code, int row)
+{
+    if (atomicCAS(&st->code, 0, code) == 0) st->row = row;
+}
+
+// Spin until *p is no longer the sentinel.  Returns false if the wait ran out
+// or another warp reported an error (the caller then leaves the kernel).
+template <typename T>
+__device__ __forceinline__ bool wait_ready(const T* p, T& out, DevStatus* st, unsigned long long budget_ns, int row)
+{
+    T v = ld_relaxed(p);
+    if (!is_pending(v)) {
+        out = v;
+        return true;
+    }
+    unsigned long long t0 = global_ns();
+    unsigned it = 0;
+    while (true) {
+        v = ld_relaxed(p);
+        if (!is_pending(v)) {
+            out = v;
+            return true;
+        }
+        if ((++it & 63u) == 0) {
+            if (ld_relaxed(&st->code) != 0) return false;
+            if (global_ns() - t0 > budget_ns) {
+                report(st, SPTRSV_ERR_TIMEOUT, row);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+}  // namespace sptrsv

@@ -1,0 +1,112 @@
+// internal.h — host-side internals shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+#include <unordered_map>
+
+#include "common.cuh"
+#include "sptrsv_b200.h"
+
+namespace sptrsv {
+
+// ---- errors --------------------------------------------------------------
+int set_error(int code, const char* fmt, ...);
+inline int ok() { return set_error(SPTRSV_OK, "ok"); }
+int cuda_fail(cudaError_t e, const char* where);
+
+#define SPT_CUDA(call)                                                        \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return ::sptrsv::cuda_fail(e_, #call);         \
+    } while (0)
+
+// ---- per-device context -------------------------------------------------
+struct Ctx {
+    int device = -1;
+    int num_sms = 0;
+    DevStatus* d_status = nullptr;  // one status block per device
+};
+Ctx* ctx();  // context of the current device (created on first use)
+unsigned long long wait_budget_ns();
+
+// Reads and clears the device status after synchronising `stream`.
+int sync_status(cudaStream_t stream);
+
+// ---- launches ------------------------------------------------------------
+// Grid for a persistent kernel: every block co-resident (occupancy x SMs),
+// capped by `max_blocks`.  Launched cooperatively so the co-residency that
+// the static round-robin schedule relies on is guaranteed by the driver.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_persistent(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks,
+                              cudaStream_t s, Args... args)
+{
+    static std::mutex mu;
+    static std::unordered_map<long long, int> occ;  // (kernel, block, smem, device) -> blocks per SM
+    Ctx* c = ctx();
+    long long key = (long long)(uintptr_t)kern ^ ((long long)block << 40) ^ ((long long)smem << 20) ^ c->device;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = occ.find(key);
+        if (it == occ.end()) {
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem);
+            if (e != cudaSuccess) return e;
+            occ[key] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+    }
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    long long grid = (long long)per_sm * c->num_sms;
+    if (max_blocks < grid) grid = max_blocks;
+    if (grid < 1) grid = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---- device primitives (util.cu) ----------------------------------------
+// Exclusive scan of m ints; in and out may alias.  Needs scratch of
+// scan_scratch_ints(m) ints.
+long long scan_scratch_ints(long long m);
+cudaError_t scan_exclusive(const int* in, int* out, long long m, int* scratch, cudaStream_t s);
+// Stable LSD radix sort of (key, val) pairs, keys in [0, max_key].  Uses the
+// *_tmp arrays as ping-pong buffers; the sorted result always ends in
+// keys/vals.  Scratch: radix_scratch_ints(n) ints.
+long long radix_scratch_ints(long long n);
+cudaError_t radix_sort_pairs(int* keys, int* vals, int* keys_tmp, int* vals_tmp, long long n, int max_key,
+                             int* scratch, cudaStream_t s);
+
+// ---- analysis record -------------------------------------------------------
+// Arrays the reference computes internally but does not put in
+// dfr_analysis_info_t; kept per analysis, keyed by the info->row_ctr device
+// pointer, which is unique per analysis and survives struct copies.
+struct AnalysisRec {
+    int device = -1;
+    int n = 0, nnz = 0, nlevs = 0, n_warps = 0;
+    int* d_levels = nullptr;   // [n] 1-based level per row
+    int* d_counts = nullptr;   // [7*nlevs+1] rows per key
+    int* d_ibase = nullptr;    // [n_warps+1] multirow map (always built)
+    int* d_ivect = nullptr;    // [n_warps]
+    int* d_wlev = nullptr;     // [n_warps]
+    bool map_in_info = false;  // map arrays are also referenced by the info struct
+};
+void register_analysis(const int* key, AnalysisRec* rec);
+AnalysisRec* find_analysis(const int* key);
+AnalysisRec* unregister_analysis(const int* key);
+
+}  // namespace sptrsv

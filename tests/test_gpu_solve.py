@@ -1,0 +1,240 @@
+"""GPU solves through the C ABI: the reference entry points and the plan
+path (FP64, FP32 + FP64 refinement, multi-RHS), against the CPU oracle,
+the reference's known-answer test and the reference's own solutions."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle import oracle as O
+from sptrsv_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # relative forward error (inf-norm) against the FP64 oracle
+
+
+def _setup(S, m, mode=None):
+    L = S.allocate_memory(m.rowptr, m.colidx, m.val, m.n)
+    info = None
+    if mode is not None:
+        info = S.AnalysisInfo()
+        info.mode = mode
+        assert S.run_analysis(info, L) == 0
+    return L, info
+
+
+MATS = {
+    "banded": lambda: gen.banded(30000, 256, 8, 8, seed=0),
+    "banded_var": lambda: gen.banded(9000, 64, 0, 24, seed=5),
+    "grid2d": lambda: gen.grid2d(160, 140, seed=1),
+    "grid3d": lambda: gen.grid3d(25, 20, 22, seed=3),
+    "zipf": lambda: gen.zipf(40000, 1.5, 256, seed=2),
+    "block": lambda: gen.blockdiag(3000, 32, seed=4),
+}
+
+
+@pytest.mark.parametrize("name", list(MATS))
+@pytest.mark.parametrize("mode", ["SIMPLE", "ORDER", "MULTIROW", "ALL"])
+def test_run_solver_host_buffers(torch_cuda, name, mode):
+    import sptrsv_b200 as S
+
+    m = MATS[name]()
+    xt = gen.vector(m.n, "uniform", seed=7)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, None if mode == "SIMPLE" else getattr(S, mode))
+    x = np.zeros(m.n)
+    S.run_solver(L, info, b, x, m.n)
+    assert O.rel_err(x, ref) <= TOL
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("name", list(MATS))
+def test_known_answer_unit_values_exact(torch_cuda, name):
+    # the reference's test input: values 1.0, b = row counts, x == 1 exactly
+    import sptrsv_b200 as S
+
+    m = MATS[name]().unit_values()
+    b = np.diff(m.rowptr).astype(np.float64)
+    L, info = _setup(S, m, S.ALL)
+    for inf in (None, info):
+        x = np.zeros(m.n)
+        S.run_solver(L, inf, b, x, m.n)
+        assert np.all(x == 1.0)
+    info.mode = S.ORDER
+    x = np.zeros(m.n)
+    S.run_solver(L, info, b, x, m.n)
+    assert np.all(x == 1.0)
+    plan = S.Plan(L, info)
+    for prec in (64, 32):
+        xp = np.zeros(m.n)
+        plan.solve_host(b, xp, 1, precision=prec)
+        assert np.all(xp == 1.0), prec
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("name", ["banded_var", "zipf", "grid2d"])
+def test_device_entry_points_and_order_tiles(torch_cuda, name):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = MATS[name]()
+    xt = gen.vector(m.n, "normal", seed=8)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    for fn in (lambda: S.csr_L_solve_simple(L, db, dx, m.n),
+               lambda: S.csr_L_solve_order(L, info, db, dx, m.n, s),
+               lambda: S.csr_L_solve_multirow(L, info, db, dx, m.n, s)):
+        dx.fill_(0)
+        fn()
+        S.sync_status(s)
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    for tile in (1, 2, 4, 8, 16, 32):
+        S.csr_L_solve_order_tile(L, info, db, dx, tile, s)
+        S.sync_status(s)
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, tile
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("name", list(MATS))
+def test_plan_variants_fp64_and_ir(torch_cuda, name):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = MATS[name]()
+    xt = gen.vector(m.n, "uniform", seed=9)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
+    for var in (S._lib.VAR_SIMPLE, S._lib.VAR_ORDER, S._lib.VAR_MULTIROW):
+        for rpw in ((1,) if var == S._lib.VAR_MULTIROW else (1, 2, 8, 32)):
+            plan.set_schedule(var, rpw, ir_max_iters=2)
+            plan.solve_f64(db, dx)
+            S.sync_status()
+            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, (var, rpw)
+            plan.solve_ir(db, dx)
+            S.sync_status()
+            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", var, rpw)
+    dr = torch.empty_like(dx)
+    plan.residual(db, dx, dr)
+    S.sync_status()
+    assert float(dr.abs().max()) <= 1e-12 * float(db.abs().max())
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 8, 16, 32])
+def test_plan_multi_rhs(torch_cuda, k):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.zipf(20000, 1.5, 256, seed=2)
+    xt = gen.vector(m.n * k, "normal", seed=10)
+    b = m.matvec(xt, k)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n * k, dtype=torch.float64, device="cuda")
+    plan.solve_f64(db, dx, k)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    plan.solve_ir(db, dx, k)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    x = np.zeros(m.n * k)
+    plan.solve_host(b, x, k, precision=32)
+    assert O.rel_err(x, ref) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+def test_value_update_reuses_analysis(torch_cuda):
+    import sptrsv_b200 as S
+
+    m = gen.banded(5000, 64, 2, 10, seed=12)
+    m2 = gen.from_arrays(m.rowptr, m.colidx, m.val * 1.5)
+    b = m2.matvec(gen.vector(m.n, "uniform", seed=3))
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    L2 = S.allocate_memory(m2.rowptr, m2.colidx, m2.val, m2.n)
+    plan.update_values(L2)
+    x = np.zeros(m.n)
+    plan.solve_host(b, x, 1, precision=64)
+    assert O.rel_err(x, O.solve(m2.rowptr, m2.colidx, m2.val, b)) <= TOL
+    plan.close()
+    S.free_device_analysis(L2, None)
+    S.free_device_analysis(L, info)
+
+
+def test_non_finite_values_complete_without_hanging(torch_cuda):
+    import sptrsv_b200 as S
+
+    m = gen.banded(2000, 32, 1, 4, seed=13)
+    val = m.val.copy()
+    val[m.rowptr[501] - 1] = 0.0  # zero diagonal in row 500 -> inf/nan downstream
+    mz = gen.from_arrays(m.rowptr, m.colidx, val)
+    b = m.matvec(np.ones(m.n))
+    ref = O.solve(mz.rowptr, mz.colidx, mz.val, b)
+    L, info = _setup(S, mz, S.MULTIROW)
+    for inf in (None, info):
+        x = np.zeros(m.n)
+        S.run_solver(L, inf, b, x, m.n)
+        assert np.array_equal(np.isfinite(x), np.isfinite(ref))
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("cfg", ["c0", "c1", "c2", "c2k16"])
+def test_full_size_configs_fp64_and_ir(torch_cuda, cfg):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m, xt, k = gen.config(cfg)
+    b = m.matvec(xt, k)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n * k, dtype=torch.float64, device="cuda")
+    plan.solve_f64(db, dx, k)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    plan.solve_ir(db, dx, k)
+    S.sync_status()
+    e = O.rel_err(dx.cpu().numpy(), ref)
+    assert e <= TOL, e
+    assert O.rel_err(dx.cpu().numpy(), xt) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+GOLDEN = golden_cases()
+
+
+@pytest.mark.skipif(not GOLDEN, reason="no golden fixtures")
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_solves_match_reference_golden(torch_cuda, path):
+    import sptrsv_b200 as S
+
+    g = load_golden(path)
+    m = gen.from_arrays(g["rowptr"], g["colidx"], g["val"])
+    L, info = _setup(S, m, S.MULTIROW)
+    for mode, inf in (("simple", None), ("multirow", info)):
+        x = np.zeros(m.n)
+        S.run_solver(L, inf, g["b"], x, m.n)
+        for v in ("simple", "order", "multirow"):
+            assert O.rel_err(x, g[f"ref_x_{v}"]) <= TOL, (mode, v)
+    plan = S.Plan(L, info)
+    x = np.zeros(m.n)
+    plan.solve_host(np.ascontiguousarray(g["b"]), x, 1, precision=32)
+    assert O.rel_err(x, g["ref_x_multirow"]) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
