@@ -198,18 +198,23 @@ int sptrsv_solve_order_tile(sp_mat_t* mat, dfr_analysis_info_t* info, const doub
 typedef struct sptrsv_plan_s* sptrsv_plan_t;
 
 /* Solve variants a schedule can pick. */
-#define SPTRSV_VAR_SIMPLE    0  /* natural row order, no analysis needed      */
-#define SPTRSV_VAR_ORDER     1  /* level order, fixed lanes per row           */
-#define SPTRSV_VAR_MULTIROW  2  /* level order, lanes per row by row length    */
-#define SPTRSV_VAR_CLUSTER   3  /* level order, block-local readiness in smem  */
+#define SPTRSV_VAR_SIMPLE    0  /* natural row order, no analysis needed            */
+#define SPTRSV_VAR_ORDER     1  /* level order, fixed lanes per row                 */
+#define SPTRSV_VAR_MULTIROW  2  /* level order, lanes per row by row length          */
+#define SPTRSV_VAR_CLUSTER   3  /* level bands cut into row clusters, one CTA each;  */
+                                /* dependencies inside a cluster through shared mem  */
 #define SPTRSV_N_VARIANTS    4
 
 typedef struct {
-    int variant;          /* SPTRSV_VAR_*                                      */
-    int rows_per_warp;    /* 1,2,4,8,16,32 (lanes per row = 32/rows_per_warp;  */
-                          /* for MULTIROW it caps the rows packed per warp)    */
-    int block_warps;      /* warps per CTA (1..32)                             */
-    int ir_max_iters;     /* FP32+IR: refinement steps after the first solve   */
+    int variant;          /* SPTRSV_VAR_*                                            */
+    int rows_per_warp;    /* 1,2,4,8,16,32: lanes per row = 32/rows_per_warp         */
+                          /* (MULTIROW takes lanes per row from the analysis map)     */
+    int block_warps;      /* warps per CTA: 2, 4, 8 or 16                             */
+    int warps_per_sm;     /* resident warps per SM of the persistent grid (0 = max)   */
+    int backoff_ns;       /* nanosleep between polls after 8 failed polls (0 = spin)  */
+    int ir_max_iters;     /* FP32+IR: refinement steps after the first FP32 solve     */
+    int band_levels;      /* CLUSTER: levels per band (H)                             */
+    int cluster_rows;     /* CLUSTER: rows per cluster (B, <= 8192)                   */
 } sptrsv_schedule_t;
 
 /* Creates a plan for the analysed matrix.  info must come from run_analysis
@@ -243,6 +248,54 @@ int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, 
 /* FP64 residual r = b - L x on the device (row-major n x nrhs). */
 int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, double* r,
                         int nrhs, cudaStream_t stream);
+
+/* --- Schedule selection: features, autotuner, learned selector ------------ */
+
+/* 12 cheap features of an analysed matrix: log2 n, log2 nnz, nnz/n,
+ * log2 nlevs, log2 mean level width, log2 max level width, the 25/50/90/99%
+ * quantiles of off-diagonals per row, log2(1 + max off-diagonals per row),
+ * fraction of diagonal-only rows. */
+int sptrsv_features(const sp_mat_t* gpu_L, const dfr_analysis_info_t* info, float* out12);
+
+/* 24 schedule classes = 4 variants x 6 parameter presets (class = 6*variant + j). */
+#define SPTRSV_N_CLASSES 24
+int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* out);
+
+/* Exhaustive autotuner: times every class on this plan (median of `reps`
+ * solves after one warm-up, L2 flushed between solves; precision 64 = plain
+ * FP64, 32 = FP32 + FP64 refinement), leaves the fastest set on the plan.
+ * b, x are DEVICE arrays (n x nrhs); times_ms[24] (may be NULL) receives each
+ * class's median, NaN for a class that could not run. */
+int sptrsv_autotune(sptrsv_plan_t plan, const double* b, double* x, int nrhs, int precision, int reps,
+                    float* times_ms, int* best_class);
+
+/* The learned selector: an MLP 12 -> 64 -> 64 -> 24 (ReLU) that predicts each
+ * class's log2(time / best time) from the features; trained and evaluated by
+ * the library's own CUDA kernels.  Parameters are 6552 floats, weights
+ * row-major [in][out]: W1[12][64] b1[64] W2[64][64] b2[64] W3[64][24] b3[24]. */
+typedef struct sptrsv_mlp_s* sptrsv_mlp_t;
+#define SPTRSV_MLP_NPARAMS 6552
+int sptrsv_mlp_create(uint64_t seed, sptrsv_mlp_t* out);
+int sptrsv_mlp_destroy(sptrsv_mlp_t mlp);
+int sptrsv_mlp_get_params(sptrsv_mlp_t mlp, float* host_params);
+int sptrsv_mlp_set_params(sptrsv_mlp_t mlp, const float* host_params);
+/* Inputs are normalised as (x - mean) / std before the first layer. */
+int sptrsv_mlp_set_normalization(sptrsv_mlp_t mlp, const float* mean12, const float* std12);
+int sptrsv_mlp_get_normalization(sptrsv_mlp_t mlp, float* mean12, float* std12);
+/* Y[B x 24] for raw features X[B x 12] (host arrays). */
+int sptrsv_mlp_forward_host(sptrsv_mlp_t mlp, const float* X, int B, float* Y);
+/* Masked MSE loss and its gradient (6552 floats) at the current parameters:
+ * L = sum M (Y - T)^2 / max(1, sum M). */
+int sptrsv_mlp_gradient_host(sptrsv_mlp_t mlp, const float* X, const float* T, const float* M, int B,
+                             float* grad, float* loss);
+/* Minibatch Adam on the device over N rows; loss_curve[epochs] may be NULL. */
+int sptrsv_mlp_train_host(sptrsv_mlp_t mlp, const float* X, const float* T, const float* M, int N, int epochs,
+                          int batch, float lr, uint64_t seed, float* loss_curve);
+/* argmin of the predicted relative times. */
+int sptrsv_mlp_predict_class(sptrsv_mlp_t mlp, const float* features12, int* cls);
+/* Features -> MLP -> schedule, set on the plan. */
+int sptrsv_plan_select_schedule(sptrsv_plan_t plan, sptrsv_mlp_t mlp, const sp_mat_t* gpu_L,
+                                const dfr_analysis_info_t* info, int* cls_out);
 
 /* --- Synthetic inputs (host code) ---------------------------------------- */
 /* The reference reads SuiteSparse .mtx files (main.cu:66-246); none ship with

@@ -53,6 +53,12 @@ def lib():
         L.oracle_num_threads.restype = c_int
         L.oracle_rel_err_inf.restype = c_double
         L.oracle_rel_err_inf.argtypes = [c_size_t, c_void_p, c_void_p]
+        L.mlp_oracle_nparams.restype = c_int
+        L.mlp_oracle_forward.restype = None
+        L.mlp_oracle_forward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]
+        L.mlp_oracle_gradient.restype = c_double
+        L.mlp_oracle_gradient.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                          c_void_p]
         _o = L
     return _o
 
@@ -122,6 +128,27 @@ def rel_err(a, b) -> float:
 
 def num_threads() -> int:
     return lib().oracle_num_threads()
+
+
+# ---- MLP oracle (oracle/mlp_oracle.c) ----
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def mlp_forward(params, mean, std, X) -> np.ndarray:
+    P, m, s, Xf = _f32(params), _f32(mean), _f32(std), _f32(X).reshape(-1, 12)
+    Y = np.zeros((Xf.shape[0], 24), dtype=np.float64)
+    lib().mlp_oracle_forward(P.ctypes.data, m.ctypes.data, s.ctypes.data, Xf.ctypes.data, Xf.shape[0], Y.ctypes.data)
+    return Y
+
+
+def mlp_gradient(params, mean, std, X, T, M):
+    P, m, s = _f32(params), _f32(mean), _f32(std)
+    Xf, Tf, Mf = _f32(X).reshape(-1, 12), _f32(T).reshape(-1, 24), _f32(M).reshape(-1, 24)
+    G = np.zeros(lib().mlp_oracle_nparams(), dtype=np.float64)
+    loss = lib().mlp_oracle_gradient(P.ctypes.data, m.ctypes.data, s.ctypes.data, Xf.ctypes.data, Tf.ctypes.data,
+                                     Mf.ctypes.data, Xf.shape[0], G.ctypes.data)
+    return loss, G
 
 
 # ---- the reference's own kernels (GPU only; built by `make -C oracle ref`) ----

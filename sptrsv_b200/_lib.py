@@ -58,7 +58,11 @@ class AnalysisInfo(ctypes.Structure):
 class Schedule(ctypes.Structure):
     """sptrsv_schedule_t."""
 
-    _fields_ = [("variant", c_int), ("rows_per_warp", c_int), ("block_warps", c_int), ("ir_max_iters", c_int)]
+    _fields_ = [("variant", c_int), ("rows_per_warp", c_int), ("block_warps", c_int), ("warps_per_sm", c_int),
+                ("backoff_ns", c_int), ("ir_max_iters", c_int), ("band_levels", c_int), ("cluster_rows", c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class HostCsr(ctypes.Structure):
@@ -98,6 +102,22 @@ _SIGS = {
     "sptrsv_solve_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "sptrsv_residual_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_features": (c_int, [POINTER(SpMat), POINTER(AnalysisInfo), c_void_p]),
+    "sptrsv_schedule_from_class": (c_int, [c_int, POINTER(Schedule)]),
+    "sptrsv_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, POINTER(c_int)]),
+    "sptrsv_mlp_create": (c_int, [c_uint64, POINTER(c_void_p)]),
+    "sptrsv_mlp_destroy": (c_int, [c_void_p]),
+    "sptrsv_mlp_get_params": (c_int, [c_void_p, c_void_p]),
+    "sptrsv_mlp_set_params": (c_int, [c_void_p, c_void_p]),
+    "sptrsv_mlp_set_normalization": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "sptrsv_mlp_get_normalization": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "sptrsv_mlp_forward_host": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_mlp_gradient_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "sptrsv_mlp_train_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, ctypes.c_float,
+                                      c_uint64, c_void_p]),
+    "sptrsv_mlp_predict_class": (c_int, [c_void_p, c_void_p, POINTER(c_int)]),
+    "sptrsv_plan_select_schedule": (c_int, [c_void_p, c_void_p, POINTER(SpMat), POINTER(AnalysisInfo),
+                                            POINTER(c_int)]),
     "sptrsv_gen_banded": (c_int, [c_int, c_int, c_int, c_int, c_uint64, POINTER(HostCsr)]),
     "sptrsv_gen_grid2d": (c_int, [c_int, c_int, c_uint64, POINTER(HostCsr)]),
     "sptrsv_gen_grid3d": (c_int, [c_int, c_int, c_int, c_uint64, POINTER(HostCsr)]),

@@ -71,6 +71,9 @@ __global__ void __launch_bounds__(256) k_levels(const int* __restrict__ rowptr, 
     const int lane = threadIdx.x & 31;
     const int R = 32 / L;
     const int seg = lane / L, sl = lane & (L - 1);
+    // consecutive rows of one task may depend on each other: each row's lanes
+    // reduce and publish under their own mask before the warp converges
+    const unsigned smask = L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (seg * L));
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long ntasks = ((long long)n + R - 1) / R;
@@ -93,12 +96,13 @@ __global__ void __launch_bounds__(256) k_levels(const int* __restrict__ rowptr, 
                 m = max(m, lv);
             }
         }
-        for (int o = L >> 1; o >= 1; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o, L));
-        if (__any_sync(0xffffffffu, fail)) return;
-        if (act && sl == 0) {
+        for (int o = L >> 1; o >= 1; o >>= 1) m = max(m, __shfl_down_sync(smask, m, o, L));
+        const bool seg_fail = __any_sync(smask, fail);
+        if (act && sl == 0 && !seg_fail) {
             st_relaxed(level + r, m + 1);
             my_max = max(my_max, m + 1);
         }
+        if (__any_sync(0xffffffffu, seg_fail)) return;
     }
     for (int o = 16; o >= 1; o >>= 1) my_max = max(my_max, __shfl_down_sync(0xffffffffu, my_max, o));
     if (lane == 0 && my_max > 0) atomicMax(nlevs, my_max);
@@ -165,32 +169,15 @@ __global__ void k_inverse(const int* __restrict__ perm, int n, int* __restrict__
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) inv[perm[k]] = k;
 }
 
-int grid_for(long long work, int block)
-{
-    long long g = (work + block - 1) / block;
-    long long cap = (long long)ctx()->num_sms * 16;
-    if (g > cap) g = cap;
-    return (int)(g < 1 ? 1 : g);
-}
 
-// lanes per row for the level kernel from nnz/n (aux_call_kernel_analysis_L_coop_groups, :216-239)
-int level_lanes(int nnz, int n)
-{
-    int average = n > 0 ? nnz / n : 0;
-    if (average <= 1) return 1;
-    if (average == 2) return 2;
-    if (average <= 5) return 4;
-    if (average <= 11) return 8;
-    if (average <= 23) return 16;
-    return 32;
-}
+// Lanes per row of the level kernel.  The reference picks a tile of 1-32
+// lanes from nnz/n (aux_call_kernel_analysis_L_coop_groups, :216-239), which
+// puts consecutive rows of the natural order in one warp; consecutive rows
+// often depend on each other, and a producer and a waiting consumer in the
+// same warp make progress only when the scheduler switches between the
+// diverged paths.  One row per warp keeps dependent rows in different warps.
+int level_lanes(int, int) { return 32; }
 
-template <typename T>
-cudaError_t dalloc(T** p, long long count)
-{
-    if (count < 1) count = 1;
-    return cudaMalloc((void**)p, sizeof(T) * (size_t)count);
-}
 
 }  // namespace
 

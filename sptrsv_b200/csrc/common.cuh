@@ -93,8 +93,11 @@ __device__ __forceinline__ void report(DevStatus* st, int code, int row)
 
 // Spin until *p is no longer the sentinel.  Returns false if the wait ran out
 // or another warp reported an error (the caller then leaves the kernel).
+// After 8 failed polls the loop sleeps `backoff_ns` between polls (0: spin),
+// which keeps far-ahead waiters from flooding L2 with polls.
 template <typename T>
-__device__ __forceinline__ bool wait_ready(const T* p, T& out, DevStatus* st, unsigned long long budget_ns, int row)
+__device__ __forceinline__ bool wait_ready(const T* p, T& out, DevStatus* st, unsigned long long budget_ns, int row,
+                                           unsigned backoff_ns = 0)
 {
     T v = ld_relaxed(p);
     if (!is_pending(v)) {
@@ -109,7 +112,9 @@ __device__ __forceinline__ bool wait_ready(const T* p, T& out, DevStatus* st, un
             out = v;
             return true;
         }
-        if ((++it & 63u) == 0) {
+        ++it;
+        if (backoff_ns && it > 8) __nanosleep(backoff_ns);
+        if ((it & 63u) == 0) {
             if (ld_relaxed(&st->code) != 0) return false;
             if (global_ns() - t0 > budget_ns) {
                 report(st, SPTRSV_ERR_TIMEOUT, row);
@@ -117,6 +122,47 @@ __device__ __forceinline__ bool wait_ready(const T* p, T& out, DevStatus* st, un
             }
         }
     }
+}
+
+// The same wait on a shared-memory slot written by another warp of the CTA.
+template <typename T>
+__device__ __forceinline__ bool wait_ready_smem(const volatile T* p, T& out, DevStatus* st,
+                                                unsigned long long budget_ns, int row)
+{
+    T v = *p;
+    if (!is_pending(v)) {
+        out = v;
+        return true;
+    }
+    unsigned long long t0 = global_ns();
+    unsigned it = 0;
+    while (true) {
+        v = *p;
+        if (!is_pending(v)) {
+            out = v;
+            return true;
+        }
+        if ((++it & 255u) == 0) {
+            if (ld_relaxed(&st->code) != 0) return false;
+            if (global_ns() - t0 > budget_ns) {
+                report(st, SPTRSV_ERR_TIMEOUT, row);
+                return false;
+            }
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T sentinel_value();
+template <>
+__device__ __forceinline__ double sentinel_value<double>()
+{
+    return __longlong_as_double(-1LL);
+}
+template <>
+__device__ __forceinline__ float sentinel_value<float>()
+{
+    return __uint_as_float(0xFFFFFFFFu);
 }
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }

@@ -38,11 +38,12 @@ int sync_status(cudaStream_t stream);
 
 // ---- launches ------------------------------------------------------------
 // Grid for a persistent kernel: every block co-resident (occupancy x SMs),
-// capped by `max_blocks`.  Launched cooperatively so the co-residency that
-// the static round-robin schedule relies on is guaranteed by the driver.
+// capped by `max_blocks` and by `cap_per_sm` blocks per SM (0: no cap).
+// Launched cooperatively so the co-residency that the static round-robin
+// schedule relies on is guaranteed by the driver.
 template <typename... KArgs, typename... Args>
-cudaError_t launch_persistent(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks,
-                              cudaStream_t s, Args... args)
+cudaError_t launch_persistent_capped(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks,
+                                     int cap_per_sm, cudaStream_t s, Args... args)
 {
     static std::mutex mu;
     static std::unordered_map<long long, int> occ;  // (kernel, block, smem, device) -> blocks per SM
@@ -61,6 +62,7 @@ cudaError_t launch_persistent(void (*kern)(KArgs...), int block, size_t smem, lo
         }
     }
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (cap_per_sm > 0 && per_sm > cap_per_sm) per_sm = cap_per_sm;
     long long grid = (long long)per_sm * c->num_sms;
     if (max_blocks < grid) grid = max_blocks;
     if (grid < 1) grid = 1;
@@ -77,7 +79,25 @@ cudaError_t launch_persistent(void (*kern)(KArgs...), int block, size_t smem, lo
     return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+template <typename... KArgs, typename... Args>
+cudaError_t launch_persistent(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks, cudaStream_t s,
+                              Args... args)
+{
+    return launch_persistent_capped(kern, block, smem, max_blocks, 0, s, args...);
+}
+
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Grid for a plain grid-stride kernel: enough blocks for `work` threads,
+// at most 16 per SM.
+int grid_for(long long work, int block);
+
+template <typename T>
+cudaError_t dalloc(T** p, long long count)
+{
+    if (count < 1) count = 1;
+    return cudaMalloc((void**)p, sizeof(T) * (size_t)count);
+}
 
 // ---- device primitives (util.cu) ----------------------------------------
 // Exclusive scan of m ints; in and out may alias.  Needs scratch of
@@ -90,6 +110,12 @@ cudaError_t scan_exclusive(const int* in, int* out, long long m, int* scratch, c
 long long radix_scratch_ints(long long n);
 cudaError_t radix_sort_pairs(int* keys, int* vals, int* keys_tmp, int* vals_tmp, long long n, int max_key,
                              int* scratch, cudaStream_t s);
+// Segment-aligned task table.  key[p] (p < n) is non-decreasing, in [0, K);
+// a segment is a run of equal keys.  Tasks are runs of at most R positions
+// inside one segment, so rows of one task never depend on each other when a
+// segment is (part of) a level.  *tbase gets ntasks+1 entries (allocated
+// here; tbase[ntasks] = n).  Returns 0 or an error code.
+int build_task_table(const int* key, int n, int K, int R, int** tbase, int* ntasks, cudaStream_t s);
 
 // ---- analysis record -------------------------------------------------------
 // Arrays the reference computes internally but does not put in
@@ -104,6 +130,8 @@ struct AnalysisRec {
     int* d_ivect = nullptr;    // [n_warps]
     int* d_wlev = nullptr;     // [n_warps]
     bool map_in_info = false;  // map arrays are also referenced by the info struct
+    int* tile_tasks[6] = {};   // level-aligned iorder tasks for 32>>j lanes per row
+    int tile_ntasks[6] = {};
 };
 void register_analysis(const int* key, AnalysisRec* rec);
 AnalysisRec* find_analysis(const int* key);

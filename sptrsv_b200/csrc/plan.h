@@ -1,24 +1,26 @@
-// plan.h — the solve plan: a level-ordered, solve-optimised copy of L.
+// plan.h — the solve plan: solve-optimised copies of L.
 //
-// HBM layout (n rows, m = nnz - n off-diagonal entries), all in iorder
-// sequence so that a warp's rows are contiguous:
+// A layout stores the rows in a schedule order so that the rows a warp (or
+// CTA) works on are contiguous (n rows, m = nnz - n off-diagonal entries):
 //   ptr[n+1]    int32   off-diagonal offsets per position
 //   rowid[n]    int32   original row of each position (b, x are indexed by it)
-//   col[m]      int32   off-diagonal column (original index)
+//   col[m]      int32   off-diagonal column (original index; in the cluster
+//                       layout ~local for a column inside the same cluster)
 //   val64[m]    f64     off-diagonal values
 //   val32[m]    f32     the same values rounded to FP32
 //   dg64[n], dg32[n]    diagonal per position
-//   inv[n]      int32   position of each original row (natural order walk)
-//   ibase[n_warps+1], ivect[n_warps]  multirow warp map (analysis copy)
+// The level layout (iorder sequence) is always built; it serves SIMPLE
+// (through inv[n], natural row -> position), ORDER, MULTIROW (with the
+// analysis warp map ibase/ivect) and the FP64 residual.  The cluster layout
+// is built when a CLUSTER schedule is set, for its (band_levels,
+// cluster_rows), with cptr[nclusters+1] giving each cluster's positions.
 // Work buffers: w32a/w32b (n x nrhs f32) for the FP32 solves and residuals,
 // hb/hx (n x nrhs f64) staging for the host-buffer entry point.
 #pragma once
 
 #include "sptrsv_b200.h"
 
-struct sptrsv_plan_s {
-    int device = -1;
-    int n = 0, nnz_off = 0, nlevs = 0, n_warps = 0;
+struct SptLayout {
     int* ptr = nullptr;
     int* rowid = nullptr;
     int* col = nullptr;
@@ -26,9 +28,25 @@ struct sptrsv_plan_s {
     float* val32 = nullptr;
     double* dg64 = nullptr;
     float* dg32 = nullptr;
-    int* inv = nullptr;
-    int* ibase = nullptr;
+};
+
+struct sptrsv_plan_s {
+    int device = -1;
+    int n = 0, nnz_off = 0, nlevs = 0, n_warps = 0;
+    SptLayout lev;               // level order
+    int* inv = nullptr;          // natural row -> level-layout position
+    int* levels = nullptr;       // 1-based level per row
+    int* ibase = nullptr;        // multirow map
     int* ivect = nullptr;
+    int* ord_tasks = nullptr;    // level-aligned tasks over the level layout
+    int ord_ntasks = 0, ord_R = 0;
+    SptLayout clu;               // cluster order (built on demand)
+    int* cptr = nullptr;
+    int* clu_key = nullptr;      // per position: cluster * H + local level
+    int nclusters = 0, clu_H = 0, clu_B = 0;
+    int* clu_tasks = nullptr;    // (cluster, level)-aligned tasks
+    int* clu_ctask = nullptr;    // first task of each cluster [nclusters+1]
+    int clu_ntasks = 0, clu_R = 0;
     float* w32a = nullptr;
     float* w32b = nullptr;
     int cap_rhs = 0;
@@ -37,3 +55,13 @@ struct sptrsv_plan_s {
     int cap_host = 0;
     sptrsv_schedule_t sched{};
 };
+
+namespace sptrsv {
+void layout_free(SptLayout& l);
+int layout_alloc(SptLayout& l, int n, int m);
+// Builds (or rebuilds) p->clu for (H, B) from the level layout.
+int build_cluster_layout(sptrsv_plan_s* p, int H, int B);
+// Level-aligned task tables with R rows per task (cached per R).
+int build_order_tasks(sptrsv_plan_s* p, int R);
+int build_cluster_tasks(sptrsv_plan_s* p, int R);
+}  // namespace sptrsv

@@ -62,6 +62,14 @@ Ctx* ctx()
 
 unsigned long long wait_budget_ns() { return g_budget_ns; }
 
+int grid_for(long long work, int block)
+{
+    long long g = (work + block - 1) / block;
+    long long cap = (long long)ctx()->num_sms * 16;
+    if (g > cap) g = cap;
+    return (int)(g < 1 ? 1 : g);
+}
+
 int sync_status(cudaStream_t stream)
 {
     Ctx* c = ctx();
@@ -278,6 +286,7 @@ void free_device_analysis(sp_mat_t* gpu_L, dfr_analysis_info_t* info)
             cudaFree(rec->d_ibase);
             cudaFree(rec->d_ivect);
             cudaFree(rec->d_wlev);
+            for (int j = 0; j < 6; j++) cudaFree(rec->tile_tasks[j]);
             delete rec;
         } else {
             cudaFree(info->ibase_row);

@@ -1,6 +1,6 @@
 // solve.cu — host side of the solves: the reference entry points
 // (header/solver.h:5-7) over the caller's CSR, and the plan API over the
-// plan's level-ordered copy (FP64, FP32 + FP64 refinement, 1-32 RHS).
+// plan's layouts (FP64, FP32 + FP64 refinement, 1-32 RHS).
 #include <cstring>
 
 #include "internal.h"
@@ -11,28 +11,36 @@ namespace sptrsv {
 
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kWarpsPerBlock = kBlock / 32;
-
-// tile lanes of the reference's simple solver from nnz/n (solve_csr_simple.cu:121-137)
-int simple_lanes(int nnz, int n)
-{
-    int average = n > 0 ? nnz / n : 0;
-    if (average <= 2) return 2;
-    if (average <= 5) return 4;
-    if (average <= 11) return 8;
-    if (average <= 23) return 16;
-    return 32;
-}
+constexpr int kRefBlock = 256;  // block of the reference-named solves
+constexpr int kRefWarps = kRefBlock / 32;
 
 bool pow2_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32; }
 
-int grid_for(long long work, int block)
+__global__ void k_iorder_level_keys(const int* __restrict__ iorder, const int* __restrict__ level, int n,
+                                    int* __restrict__ key)
 {
-    long long g = (work + block - 1) / block;
-    long long cap = (long long)ctx()->num_sms * 16;
-    if (g > cap) g = cap;
-    return (int)(g < 1 ? 1 : g);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) key[p] = level[iorder[p]] - 1;
+}
+
+// Level-aligned tasks over iorder for `lanes` lanes per row, cached with the analysis.
+int tile_tasks(AnalysisRec* rec, const int* iorder, int lanes, const int** tasks, int* ntasks)
+{
+    int j = 0;
+    while ((32 >> j) != lanes) j++;
+    if (!rec->tile_tasks[j]) {
+        int* key = nullptr;
+        SPT_CUDA(dalloc(&key, rec->n));
+        k_iorder_level_keys<<<grid_for(rec->n, 256), 256>>>(iorder, rec->d_levels, rec->n, key);
+        cudaError_t ce = cudaGetLastError();
+        int e = ce == cudaSuccess ? build_task_table(key, rec->n, rec->nlevs > 0 ? rec->nlevs : 1, 32 / lanes,
+                                                      &rec->tile_tasks[j], &rec->tile_ntasks[j], 0)
+                                  : cuda_fail(ce, "tile tasks");
+        cudaFree(key);
+        if (e) return e;
+    }
+    *tasks = rec->tile_tasks[j];
+    *ntasks = rec->tile_ntasks[j];
+    return 0;
 }
 
 }  // namespace
@@ -64,14 +72,27 @@ int solve_reference(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b, d
             ivect = rec->d_ivect;
             nw = rec->n_warps;
         }
-        SPT_CUDA(launch_persistent(kern, kBlock, 0, div_up(nw, kWarpsPerBlock), s, m, n, nw, 0, ibase, ivect, b, x,
-                                   (double*)nullptr, c->d_status, budget));
+        SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(nw, kRefWarps), s, m, n, nw, 0, ibase, ivect, b, x,
+                                   (double*)nullptr, c->d_status, budget, 0u));
+    } else if (mode == ORDER && lanes && lanes < 32) {
+        // order with a tile of `lanes` lanes: tasks never cross a level, so the
+        // rows of one warp are independent
+        AnalysisRec* rec = find_analysis(info->row_ctr);
+        if (!rec) return set_error(SPTRSV_ERR_NOT_ANALYSED, "solve: no analysis record for this info");
+        const int* tasks = nullptr;
+        int ntasks = 0;
+        int e = tile_tasks(rec, info->iorder, lanes, &tasks, &ntasks);
+        if (e) return e;
+        SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(ntasks, kRefWarps), s, m, n, ntasks, lanes, tasks,
+                                   (const int*)nullptr, b, x, (double*)nullptr, c->d_status, budget, 0u));
     } else {
-        int L = lanes ? lanes : (mode == SIMPLE ? simple_lanes(mat->nnz, n) : 32);
+        // SIMPLE walks the natural order: one row per warp by default, so that
+        // consecutive (often dependent) rows never share a warp
+        int L = lanes ? lanes : 32;
         int ntasks = div_up(n, 32 / L);
-        SPT_CUDA(launch_persistent(kern, kBlock, 0, div_up(ntasks, kWarpsPerBlock), s, m, n, ntasks, L,
+        SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(ntasks, kRefWarps), s, m, n, ntasks, L,
                                    (const int*)nullptr, (const int*)nullptr, b, x, (double*)nullptr, c->d_status,
-                                   budget));
+                                   budget, 0u));
     }
     return ok();
 }
@@ -95,41 +116,56 @@ __global__ void k_plan_rows(const int* __restrict__ rowptr, const int* __restric
 }
 
 // one warp per position copies the row's off-diagonal entries and diagonal
-__global__ void k_plan_fill(const int* __restrict__ rowptr, const int* __restrict__ col, const double* __restrict__ val,
-                            const int* __restrict__ rowid, const int* __restrict__ ptr, int n, int* __restrict__ pcol,
-                            double* __restrict__ pval, float* __restrict__ pval32, double* __restrict__ dg,
-                            float* __restrict__ dg32)
+__global__ void k_plan_fill(const int* __restrict__ rowptr, const int* __restrict__ col,
+                            const double* __restrict__ val, SptLayout l, int n)
 {
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long k = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
-        int r = rowid[k];
-        int s = rowptr[r], e = rowptr[r + 1] - 1, o = ptr[k];
+        int r = l.rowid[k];
+        int s = rowptr[r], e = rowptr[r + 1] - 1, o = l.ptr[k];
         for (int p = s + lane; p < e; p += 32) {
             double v = val[p];
-            pcol[o + p - s] = col[p];
-            if (pval) pval[o + p - s] = v;
-            pval32[o + p - s] = (float)v;
+            l.col[o + p - s] = col[p];
+            l.val64[o + p - s] = v;
+            l.val32[o + p - s] = (float)v;
         }
         if (lane == 0) {
-            dg[k] = val[e];
-            dg32[k] = (float)val[e];
+            l.dg64[k] = val[e];
+            l.dg32[k] = (float)val[e];
         }
     }
 }
 
-template <typename T>
-cudaError_t dalloc(T** p, long long count)
-{
-    if (count < 1) count = 1;
-    return cudaMalloc((void**)p, sizeof(T) * (size_t)count);
-}
-
 void plan_free_arrays(sptrsv_plan_s* p)
 {
-    cudaFree(p->ptr); cudaFree(p->rowid); cudaFree(p->col); cudaFree(p->val64); cudaFree(p->val32);
-    cudaFree(p->dg64); cudaFree(p->dg32); cudaFree(p->inv); cudaFree(p->ibase); cudaFree(p->ivect);
+    layout_free(p->lev);
+    layout_free(p->clu);
+    cudaFree(p->cptr); cudaFree(p->inv); cudaFree(p->levels); cudaFree(p->ibase); cudaFree(p->ivect);
+    cudaFree(p->ord_tasks); cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
     cudaFree(p->w32a); cudaFree(p->w32b); cudaFree(p->hb); cudaFree(p->hx);
+}
+
+sptrsv_schedule_t default_schedule()
+{
+    sptrsv_schedule_t s;
+    s.variant = SPTRSV_VAR_MULTIROW;
+    s.rows_per_warp = 1;
+    s.block_warps = 8;
+    s.warps_per_sm = 0;
+    s.backoff_ns = 0;
+    s.ir_max_iters = 2;
+    s.band_levels = 64;
+    s.cluster_rows = 4096;
+    return s;
+}
+
+// Once-per-instantiation opt-in to large dynamic shared memory.
+template <typename K>
+cudaError_t allow_smem(K kern, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 }  // namespace
@@ -137,9 +173,15 @@ void plan_free_arrays(sptrsv_plan_s* p)
 int plan_fill_values(sptrsv_plan_s* p, const sp_mat_t* L, cudaStream_t s)
 {
     if (p->n == 0) return 0;
-    k_plan_fill<<<grid_for((long long)p->n * 32, kBlock), kBlock, 0, s>>>(L->ia, L->ja, L->a, p->rowid, p->ptr, p->n,
-                                                                          p->col, p->val64, p->val32, p->dg64, p->dg32);
+    k_plan_fill<<<grid_for((long long)p->n * 32, 256), 256, 0, s>>>(L->ia, L->ja, L->a, p->lev, p->n);
     SPT_CUDA(cudaGetLastError());
+    if (p->clu.ptr) {  // rebuild the cluster copy from the new values
+        int H = p->clu_H, B = p->clu_B;
+        p->clu_H = 0;
+        SPT_CUDA(cudaStreamSynchronize(s));
+        int e = build_cluster_layout(p, H, B);
+        if (e) return e;
+    }
     return 0;
 }
 
@@ -156,33 +198,73 @@ int plan_ensure_work(sptrsv_plan_s* p, int nrhs)
     return 0;
 }
 
-// Launch one sync-free solve over the plan layout.
+// One sync-free solve over the plan: FP64 (V = T = double) or FP32.
 template <typename V, typename T, typename BT, int OUT>
-int plan_launch(sptrsv_plan_s* p, const V* val, const V* dg, const BT* b, T* x, double* x64, int nrhs, cudaStream_t s)
+int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int nrhs, cudaStream_t s)
 {
     Ctx* c = ctx();
     const sptrsv_schedule_t& sc = p->sched;
-    PermMat<V> m{p->ptr, p->rowid, p->col, val, dg, sc.variant == SPTRSV_VAR_SIMPLE ? p->inv : nullptr};
     const unsigned long long budget = wait_budget_ns();
+    const unsigned backoff = (unsigned)sc.backoff_ns;
     const int n = p->n;
+    const int block = 32 * sc.block_warps;
+    const int cap = sc.warps_per_sm > 0 ? (sc.warps_per_sm + sc.block_warps - 1) / sc.block_warps : 0;
+    auto layout_vals = [&](const SptLayout& l, const V*& val, const V*& dg) {
+        if (f32) {
+            val = reinterpret_cast<const V*>(l.val32);
+            dg = reinterpret_cast<const V*>(l.dg32);
+        } else {
+            val = reinterpret_cast<const V*>(l.val64);
+            dg = reinterpret_cast<const V*>(l.dg64);
+        }
+    };
+    if (sc.variant == SPTRSV_VAR_CLUSTER && nrhs == 1) {
+        int e = build_cluster_layout(p, sc.band_levels, sc.cluster_rows);
+        if (!e) e = build_cluster_tasks(p, sc.rows_per_warp);
+        if (e) return e;
+        const V *val, *dg;
+        layout_vals(p->clu, val, dg);
+        PermMat<V> m{p->clu.ptr, p->clu.rowid, p->clu.col, val, dg, nullptr};
+        auto kern = k_sptrsv_cluster<V, T, BT, OUT>;
+        size_t smem = sizeof(T) * (size_t)p->clu_B;
+        SPT_CUDA(allow_smem(kern, smem));
+        SPT_CUDA(launch_persistent_capped(kern, block, smem, p->nclusters, cap, s, m, (const int*)p->cptr,
+                                          (const int*)p->clu_ctask, (const int*)p->clu_tasks, p->nclusters,
+                                          32 / sc.rows_per_warp, b, x, x64, c->d_status, budget, backoff));
+        return 0;
+    }
+    const V *val, *dg;
+    layout_vals(p->lev, val, dg);
+    PermMat<V> m{p->lev.ptr, p->lev.rowid, p->lev.col, val, dg,
+                 sc.variant == SPTRSV_VAR_SIMPLE ? p->inv : nullptr};
+    const int wpb = sc.block_warps;
     if (nrhs > 1) {
         int kp = 1;
         while (kp < nrhs) kp <<= 1;
         int ntasks = div_up(n, 32 / kp);
         auto kern = k_sptrsv_mrhs<PermMat<V>, T, BT, OUT>;
-        SPT_CUDA(launch_persistent(kern, kBlock, 0, div_up(ntasks, kWarpsPerBlock), s, m, n, nrhs, kp, b, x, x64,
-                                   c->d_status, budget));
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(ntasks, wpb), cap, s, m, n, nrhs, kp, b, x, x64,
+                                          c->d_status, budget, backoff));
         return 0;
     }
     auto kern = k_sptrsv<PermMat<V>, T, BT, OUT>;
     if (sc.variant == SPTRSV_VAR_MULTIROW) {
-        SPT_CUDA(launch_persistent(kern, kBlock, 0, div_up(p->n_warps, kWarpsPerBlock), s, m, n, p->n_warps, 0,
-                                   (const int*)p->ibase, (const int*)p->ivect, b, x, x64, c->d_status, budget));
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->n_warps, wpb), cap, s, m, n, p->n_warps, 0,
+                                          (const int*)p->ibase, (const int*)p->ivect, b, x, x64, c->d_status, budget,
+                                          backoff));
+    } else if (sc.variant == SPTRSV_VAR_ORDER) {
+        // level-aligned tasks: rows of one warp never depend on each other
+        int e = build_order_tasks(p, sc.rows_per_warp);
+        if (e) return e;
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->ord_ntasks, wpb), cap, s, m, n, p->ord_ntasks,
+                                          32 / sc.rows_per_warp, (const int*)p->ord_tasks, (const int*)nullptr, b, x,
+                                          x64, c->d_status, budget, backoff));
     } else {
         int L = 32 / sc.rows_per_warp;
         int ntasks = div_up(n, sc.rows_per_warp);
-        SPT_CUDA(launch_persistent(kern, kBlock, 0, div_up(ntasks, kWarpsPerBlock), s, m, n, ntasks, L,
-                                   (const int*)nullptr, (const int*)nullptr, b, x, x64, c->d_status, budget));
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(ntasks, wpb), cap, s, m, n, ntasks, L,
+                                          (const int*)nullptr, (const int*)nullptr, b, x, x64, c->d_status, budget,
+                                          backoff));
     }
     return 0;
 }
@@ -190,20 +272,20 @@ int plan_launch(sptrsv_plan_s* p, const V* val, const V* dg, const BT* b, T* x, 
 int plan_residual(sptrsv_plan_s* p, const double* b, const double* x, float* r32, double* r64, int nrhs,
                   cudaStream_t s)
 {
-    PermMat<double> m{p->ptr, p->rowid, p->col, p->val64, p->dg64, nullptr};
+    PermMat<double> m{p->lev.ptr, p->lev.rowid, p->lev.col, p->lev.val64, p->lev.dg64, nullptr};
     const int n = p->n;
     if (nrhs > 1) {
         int kp = 1;
         while (kp < nrhs) kp <<= 1;
         long long work = (long long)div_up(n, 32 / kp) * 32;
-        if (r32) k_residual_mrhs<float><<<grid_for(work, kBlock), kBlock, 0, s>>>(m, n, nrhs, kp, b, x, r32);
-        else k_residual_mrhs<double><<<grid_for(work, kBlock), kBlock, 0, s>>>(m, n, nrhs, kp, b, x, r64);
+        if (r32) k_residual_mrhs<float><<<grid_for(work, 256), 256, 0, s>>>(m, n, nrhs, kp, b, x, r32);
+        else k_residual_mrhs<double><<<grid_for(work, 256), 256, 0, s>>>(m, n, nrhs, kp, b, x, r64);
     } else {
         int avg = n > 0 ? p->nnz_off / n : 0;
         int L = avg <= 1 ? 1 : avg <= 2 ? 2 : avg <= 4 ? 4 : avg <= 8 ? 8 : avg <= 16 ? 16 : 32;
         long long work = (long long)div_up(n, 32 / L) * 32;
-        if (r32) k_residual<float><<<grid_for(work, kBlock), kBlock, 0, s>>>(m, n, L, b, x, r32);
-        else k_residual<double><<<grid_for(work, kBlock), kBlock, 0, s>>>(m, n, L, b, x, r64);
+        if (r32) k_residual<float><<<grid_for(work, 256), 256, 0, s>>>(m, n, L, b, x, r32);
+        else k_residual<double><<<grid_for(work, 256), 256, 0, s>>>(m, n, L, b, x, r64);
     }
     SPT_CUDA(cudaGetLastError());
     return 0;
@@ -212,7 +294,7 @@ int plan_residual(sptrsv_plan_s* p, const double* b, const double* x, float* r32
 int plan_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s)
 {
     SPT_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(double) * (size_t)p->n * nrhs, s));
-    return plan_launch<double, double, double, OUT_X>(p, p->val64, p->dg64, b, x, nullptr, nrhs, s);
+    return plan_launch<double, double, double, OUT_X>(p, false, b, x, nullptr, nrhs, s);
 }
 
 int plan_solve_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s)
@@ -221,15 +303,31 @@ int plan_solve_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaSt
     if (e) return e;
     const size_t bytes32 = sizeof(float) * (size_t)p->n * nrhs;
     SPT_CUDA(cudaMemsetAsync(p->w32a, 0xFF, bytes32, s));
-    e = plan_launch<float, float, double, OUT_SET64>(p, p->val32, p->dg32, b, p->w32a, x, nrhs, s);
+    e = plan_launch<float, float, double, OUT_SET64>(p, true, b, p->w32a, x, nrhs, s);
     if (e) return e;
     for (int it = 0; it < p->sched.ir_max_iters; it++) {
         e = plan_residual(p, b, x, p->w32b, nullptr, nrhs, s);
         if (e) return e;
         SPT_CUDA(cudaMemsetAsync(p->w32a, 0xFF, bytes32, s));
-        e = plan_launch<float, float, float, OUT_ADD64>(p, p->val32, p->dg32, p->w32b, p->w32a, x, nrhs, s);
+        e = plan_launch<float, float, float, OUT_ADD64>(p, true, p->w32b, p->w32a, x, nrhs, s);
         if (e) return e;
     }
+    return 0;
+}
+
+int check_schedule(const sptrsv_schedule_t* s)
+{
+    if (s->variant < 0 || s->variant >= SPTRSV_N_VARIANTS)
+        return set_error(SPTRSV_ERR_UNSUPPORTED, "schedule: unknown variant %d", s->variant);
+    if (!pow2_lanes(s->rows_per_warp)) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: rows_per_warp");
+    if (s->block_warps != 2 && s->block_warps != 4 && s->block_warps != 8 && s->block_warps != 16)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: block_warps must be 2, 4, 8 or 16");
+    if (s->warps_per_sm < 0 || s->warps_per_sm > 64) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: warps_per_sm");
+    if (s->backoff_ns < 0 || s->backoff_ns > 100000) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: backoff_ns");
+    if (s->ir_max_iters < 0 || s->ir_max_iters > 16) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: ir_max_iters");
+    if (s->band_levels < 1 || s->band_levels > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: band_levels");
+    if (s->cluster_rows < 32 || s->cluster_rows > 8192)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: cluster_rows must be in [32, 8192]");
     return 0;
 }
 
@@ -280,6 +378,7 @@ int sptrsv_plan_create(const sp_mat_t* L, const dfr_analysis_info_t* info, sptrs
     p->nnz_off = L->nnz - L->nr;
     p->nlevs = rec->nlevs;
     p->n_warps = rec->n_warps;
+    p->sched = default_schedule();
     const int n = p->n;
     int* d_scr = nullptr;
     auto fail = [&](int code) {
@@ -293,24 +392,23 @@ int sptrsv_plan_create(const sp_mat_t* L, const dfr_analysis_info_t* info, sptrs
         cudaError_t e_ = (call);                                  \
         if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
     } while (0)
-    PCHK(dalloc(&p->ptr, (long long)n + 1));
-    PCHK(dalloc(&p->rowid, n));
-    PCHK(dalloc(&p->col, p->nnz_off));
-    PCHK(dalloc(&p->val64, p->nnz_off));
-    PCHK(dalloc(&p->val32, p->nnz_off));
-    PCHK(dalloc(&p->dg64, n));
-    PCHK(dalloc(&p->dg32, n));
+    {
+        int e = layout_alloc(p->lev, n, p->nnz_off);
+        if (e) return fail(e);
+    }
     PCHK(dalloc(&p->inv, n));
+    PCHK(dalloc(&p->levels, n));
     PCHK(dalloc(&p->ibase, (long long)p->n_warps + 1));
     PCHK(dalloc(&p->ivect, p->n_warps));
     PCHK(dalloc(&d_scr, scan_scratch_ints((long long)n + 1)));
     if (n > 0) {
-        k_plan_rows<<<grid_for((long long)n + 1, kBlock), kBlock, 0, s>>>(L->ia, info->iorder, n, p->ptr, p->rowid);
+        k_plan_rows<<<grid_for((long long)n + 1, 256), 256, 0, s>>>(L->ia, info->iorder, n, p->lev.ptr, p->lev.rowid);
         PCHK(cudaGetLastError());
-        PCHK(scan_exclusive(p->ptr, p->ptr, (long long)n + 1, d_scr, s));
+        PCHK(scan_exclusive(p->lev.ptr, p->lev.ptr, (long long)n + 1, d_scr, s));
         int e = plan_fill_values(p, L, s);
         if (e) return fail(e);
         PCHK(cudaMemcpyAsync(p->inv, info->inv_iorder, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        PCHK(cudaMemcpyAsync(p->levels, rec->d_levels, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
     }
     PCHK(cudaMemcpyAsync(p->ibase, rec->d_ibase, sizeof(int) * ((size_t)p->n_warps + 1), cudaMemcpyDeviceToDevice, s));
     if (p->n_warps > 0)
@@ -318,10 +416,6 @@ int sptrsv_plan_create(const sp_mat_t* L, const dfr_analysis_info_t* info, sptrs
     PCHK(cudaStreamSynchronize(s));
 #undef PCHK
     cudaFree(d_scr);
-    p->sched.variant = SPTRSV_VAR_MULTIROW;
-    p->sched.rows_per_warp = 1;
-    p->sched.block_warps = kWarpsPerBlock;
-    p->sched.ir_max_iters = 2;
     *out = p;
     return ok();
 }
@@ -337,12 +431,17 @@ int sptrsv_plan_destroy(sptrsv_plan_t p)
 int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
 {
     if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: NULL argument");
-    if (s->variant < 0 || s->variant >= SPTRSV_N_VARIANTS || s->variant == SPTRSV_VAR_CLUSTER)
-        return set_error(SPTRSV_ERR_UNSUPPORTED, "set_schedule: variant %d not available", s->variant);
-    if (!pow2_lanes(s->rows_per_warp)) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: rows_per_warp");
-    if (s->ir_max_iters < 0 || s->ir_max_iters > 16) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: ir_max_iters");
+    int e = check_schedule(s);
+    if (e) return e;
+    if (s->variant == SPTRSV_VAR_CLUSTER) {
+        e = build_cluster_layout(p, s->band_levels, s->cluster_rows);
+        if (!e) e = build_cluster_tasks(p, s->rows_per_warp);
+        if (e) return e;
+    } else if (s->variant == SPTRSV_VAR_ORDER) {
+        e = build_order_tasks(p, s->rows_per_warp);
+        if (e) return e;
+    }
     p->sched = *s;
-    p->sched.block_warps = kWarpsPerBlock;
     return ok();
 }
 
@@ -384,7 +483,7 @@ int sptrsv_solve_f32(sptrsv_plan_t p, const double* b, float* x32, int nrhs, cud
     if (!p || !b || !x32 || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f32: bad arguments");
     if (p->n == 0) return ok();
     SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)p->n * nrhs, stream));
-    int e = plan_launch<float, float, double, OUT_X>(p, p->val32, p->dg32, b, x32, nullptr, nrhs, stream);
+    int e = plan_launch<float, float, double, OUT_X>(p, true, b, x32, nullptr, nrhs, stream);
     return e ? e : ok();
 }
 

@@ -9,17 +9,19 @@
 // (solve_csr_multirow.cu:56-59).
 //
 // Scheduling: a persistent, co-resident grid; task t goes to warp t mod W
-// and every warp walks its tasks in increasing order.  Tasks are laid out
-// in a topological order (level order, or natural row order), so the
-// lowest unfinished task never waits on anything unfinished: no deadlock and
-// no ticket atomics (the reference takes one global atomicAdd per warp,
+// (cluster c to CTA c mod G) and every warp walks its tasks in increasing
+// order.  Tasks are laid out in a topological order, so the lowest
+// unfinished task never waits on anything unfinished: no deadlock and no
+// ticket atomics (the reference takes one global atomicAdd per warp,
 // solve_csr_order.cu:224).
 //
 // Matrix access goes through a layout policy:
 //   NatMat   — the caller's CSR (ia, ja, a) plus an optional row sequence
 //              (iorder), exactly the data the reference kernels read;
-//   PermMat  — the plan's copy: rows stored in level order, off-diagonal
-//              entries only (diagonal split out), FP64 or FP32 values.
+//   PermMat  — the plan's copy: rows stored in schedule order, off-diagonal
+//              entries only (diagonal split out), FP64 or FP32 values.  In
+//              the cluster layout a column c < 0 names the row at local
+//              position ~c of the same cluster (its value is in shared memory).
 #pragma once
 
 #include "common.cuh"
@@ -55,12 +57,12 @@ struct NatMat {
 
 template <typename VT>
 struct PermMat {
-    const int* __restrict__ ptr;    // [n+1] off-diagonal offsets, level order
+    const int* __restrict__ ptr;    // [n+1] off-diagonal offsets per position
     const int* __restrict__ rowid;  // [n] original row of each position
     const int* __restrict__ col;    // off-diagonal columns (original indices)
     const VT* __restrict__ val;     // off-diagonal values
     const VT* __restrict__ dg;      // [n] diagonal per position
-    const int* __restrict__ seq;    // null: level order; else natural -> position
+    const int* __restrict__ seq;    // null: layout order; else natural -> position
     typedef VT V;
     __device__ __forceinline__ RowRef row(int pos) const
     {
@@ -88,15 +90,22 @@ __device__ __forceinline__ void publish(T* x, double* x64, size_t i, T v)
     if (OUT == OUT_ADD64) x64[i] += (double)v;
 }
 
+__device__ __forceinline__ unsigned segment_mask(int L, int seg)
+{
+    return L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (seg * L));
+}
+
 // Single right-hand side.  Task t: `lanes` lanes per row, 32/lanes rows.
-// Fixed lanes (task_base == null): task t covers positions [t*R, t*R+R).
-// Multirow map: task t covers [task_base[t], task_base[t+1]) with
-// task_lanes[t] lanes per row (0: diagonal-only rows, one lane each).
+// No table: task t covers positions [t*R, t*R+R) with fixed lanes.
+// Table: task t covers [task_base[t], task_base[t+1]) with task_lanes[t]
+// lanes per row (the multirow map; 0: diagonal-only rows, one lane each) or,
+// when task_lanes is null, with fixed lanes (level-aligned tasks).
 template <class M, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(256) k_sptrsv(M m, int npos, int ntasks, int fixed_lanes,
+__global__ void __launch_bounds__(512) k_sptrsv(M m, int npos, int ntasks, int fixed_lanes,
                                                 const int* __restrict__ task_base,
                                                 const int* __restrict__ task_lanes, const BT* __restrict__ b, T* x,
-                                                double* x64, DevStatus* st, unsigned long long budget)
+                                                double* x64, DevStatus* st, unsigned long long budget,
+                                                unsigned backoff)
 {
     const int lane = threadIdx.x & 31;
     const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -106,7 +115,7 @@ __global__ void __launch_bounds__(256) k_sptrsv(M m, int npos, int ntasks, int f
         if (task_base) {
             base = __ldg(task_base + t);
             cnt = __ldg(task_base + t + 1) - base;
-            L = __ldg(task_lanes + t);
+            L = task_lanes ? __ldg(task_lanes + t) : fixed_lanes;
         } else {
             L = fixed_lanes;
             base = t * (32 / L);
@@ -120,7 +129,11 @@ __global__ void __launch_bounds__(256) k_sptrsv(M m, int npos, int ntasks, int f
             }
             continue;
         }
+        // Rows of one task may depend on each other (fixed lanes over level or
+        // natural order), so each row's lanes reduce and publish on their own
+        // (segment mask); the warp converges only after every row published.
         const int seg = lane / L, sl = lane & (L - 1);
+        const unsigned smask = segment_mask(L, seg);
         const bool act = seg < cnt;
         T acc = 0;
         bool fail = false;
@@ -134,24 +147,93 @@ __global__ void __launch_bounds__(256) k_sptrsv(M m, int npos, int ntasks, int f
                 int c = m.c(p);
                 T v = (T)m.v(p);
                 T xv;
-                if (!wait_ready(x + c, xv, st, budget, q.r)) {
+                if (!wait_ready(x + c, xv, st, budget, q.r, backoff)) {
                     fail = true;
                     break;
                 }
                 acc -= v * xv;
             }
         }
-        for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, L);
-        if (__any_sync(0xffffffffu, fail)) return;
-        if (act && sl == 0) publish<T, OUT>(x, x64, q.r, acc * piv);
+        for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
+        const bool seg_fail = __any_sync(smask, fail);
+        if (act && sl == 0 && !seg_fail) publish<T, OUT>(x, x64, q.r, acc * piv);
+        if (__any_sync(0xffffffffu, seg_fail)) return;
+    }
+}
+
+// Cluster schedule: CTA g processes clusters g, g+G, ...; cluster c holds the
+// positions [cptr[c], cptr[c+1]) in level order and the level-aligned tasks
+// [ctask[c], ctask[c+1]) (task t: positions [tbase[t], tbase[t+1])).  The
+// CTA's warps walk the cluster's tasks round-robin; a dependency inside the
+// cluster is read from shared memory (the slot is the flag, filled with the
+// sentinel when the cluster starts), one outside it from x in global memory.
+template <typename V, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(512) k_sptrsv_cluster(PermMat<V> m, const int* __restrict__ cptr,
+                                                        const int* __restrict__ ctask, const int* __restrict__ tbase,
+                                                        int nclusters, int L, const BT* __restrict__ b, T* x,
+                                                        double* x64, DevStatus* st, unsigned long long budget,
+                                                        unsigned backoff)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    volatile T* xs = reinterpret_cast<volatile T*>(smem_raw);
+    __shared__ int abort_flag;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+    const int seg = lane / L, sl = lane & (L - 1);
+    const unsigned smask = segment_mask(L, seg);
+    for (int c = blockIdx.x; c < nclusters; c += gridDim.x) {
+        const int cs = __ldg(cptr + c), cn = __ldg(cptr + c + 1) - cs;
+        for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = sentinel_value<T>();
+        if (threadIdx.x == 0) abort_flag = 0;
+        __syncthreads();
+        const int t0 = __ldg(ctask + c), t1 = __ldg(ctask + c + 1);
+        for (int t = t0 + wib; t < t1; t += nwb) {
+            const int tb = __ldg(tbase + t), tcnt = __ldg(tbase + t + 1) - tb;
+            const int loc = tb - cs + seg;
+            const bool act = seg < tcnt;
+            T acc = 0;
+            bool fail = false;
+            RowRef q;
+            T piv = 0;
+            if (act) {
+                q = m.row(cs + loc);
+                piv = (T)1 / (T)m.diag(q);
+                if (sl == 0) acc = (T)b[q.r];
+                for (int p = q.s + sl; p < q.e; p += L) {
+                    int cc = m.c(p);
+                    T v = (T)m.v(p);
+                    T xv;
+                    bool okw = cc < 0 ? wait_ready_smem(xs + (~cc), xv, st, budget, q.r)
+                                      : wait_ready(x + cc, xv, st, budget, q.r, backoff);
+                    if (!okw) {
+                        fail = true;
+                        break;
+                    }
+                    acc -= v * xv;
+                }
+            }
+            for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
+            const bool seg_fail = __any_sync(smask, fail);
+            if (act && sl == 0 && !seg_fail) {
+                T val = publishable(acc * piv);
+                xs[loc] = val;
+                publish<T, OUT>(x, x64, q.r, val);
+            }
+            if (__any_sync(0xffffffffu, seg_fail)) {
+                if (lane == 0) abort_flag = 1;
+                break;
+            }
+        }
+        __syncthreads();
+        if (abort_flag) return;
     }
 }
 
 // nrhs right-hand sides (row-major n x K).  kp = power of two >= K lanes per
 // row, 32/kp rows per task; lane k of a row owns right-hand side k.
 template <class M, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(256) k_sptrsv_mrhs(M m, int npos, int K, int kp, const BT* __restrict__ b, T* x,
-                                                     double* x64, DevStatus* st, unsigned long long budget)
+__global__ void __launch_bounds__(512) k_sptrsv_mrhs(M m, int npos, int K, int kp, const BT* __restrict__ b, T* x,
+                                                     double* x64, DevStatus* st, unsigned long long budget,
+                                                     unsigned backoff)
 {
     const int lane = threadIdx.x & 31;
     const int R = 32 / kp;
@@ -171,7 +253,7 @@ __global__ void __launch_bounds__(256) k_sptrsv_mrhs(M m, int npos, int K, int k
                 int c = m.c(p);
                 T v = (T)m.v(p);
                 T xv;
-                if (!wait_ready(x + (size_t)c * K + k, xv, st, budget, q.r)) {
+                if (!wait_ready(x + (size_t)c * K + k, xv, st, budget, q.r, backoff)) {
                     fail = true;
                     break;
                 }
@@ -183,8 +265,8 @@ __global__ void __launch_bounds__(256) k_sptrsv_mrhs(M m, int npos, int K, int k
     }
 }
 
-// FP64 residual r = b - L x over the plan layout; L lanes per row
-// (single RHS) or one lane per right-hand side (K > 1, rows in order).
+// FP64 residual r = b - L x over a plan layout (columns must be global);
+// L lanes per row (single RHS) or one lane per right-hand side (K > 1).
 template <typename RT>
 __global__ void __launch_bounds__(256) k_residual(PermMat<double> m, int npos, int L, const double* __restrict__ b,
                                                   const double* __restrict__ x, RT* __restrict__ r)

@@ -208,7 +208,76 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const int* __re
     }
 }
 
+__global__ void k_seg_count(const int* __restrict__ key, int n, int* __restrict__ cnt)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int k = key[p];
+        unsigned peers = __match_any_sync(__activemask(), k);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + k, __popc(peers));
+    }
+}
+
+__global__ void k_task_flags(const int* __restrict__ key, const int* __restrict__ seg_ptr, int n, int R,
+                             int* __restrict__ flag)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x)
+        flag[p] = p < n ? ((p - seg_ptr[key[p]]) % R == 0) : 0;
+}
+
+__global__ void k_task_base(const int* __restrict__ flag_scan, const int* __restrict__ key,
+                            const int* __restrict__ seg_ptr, int n, int R, int* __restrict__ tbase)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x) {
+        if (p == n) tbase[flag_scan[n]] = n;
+        else if ((p - seg_ptr[key[p]]) % R == 0) tbase[flag_scan[p]] = p;
+    }
+}
+
 }  // namespace
+
+int build_task_table(const int* key, int n, int K, int R, int** tbase, int* ntasks, cudaStream_t s)
+{
+    *tbase = nullptr;
+    *ntasks = 0;
+    int *cnt = nullptr, *flag = nullptr, *scr = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(cnt);
+        cudaFree(flag);
+        cudaFree(scr);
+    };
+#define TCHK(call)                                   \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) {                     \
+            cleanup();                               \
+            return cuda_fail(e_, #call);             \
+        }                                            \
+    } while (0)
+    long long sn = scan_scratch_ints((long long)(n > K ? n : K) + 1);
+    TCHK(dalloc(&cnt, (long long)K + 1));
+    TCHK(dalloc(&flag, (long long)n + 1));
+    TCHK(dalloc(&scr, sn));
+    TCHK(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)K + 1), s));
+    if (n > 0) {
+        k_seg_count<<<grid_for(n, 256), 256, 0, s>>>(key, n, cnt);
+        TCHK(cudaGetLastError());
+    }
+    TCHK(scan_exclusive(cnt, cnt, (long long)K + 1, scr, s));  // cnt -> segment starts
+    k_task_flags<<<grid_for((long long)n + 1, 256), 256, 0, s>>>(key, cnt, n, R, flag);
+    TCHK(cudaGetLastError());
+    TCHK(scan_exclusive(flag, flag, (long long)n + 1, scr, s));
+    int nt = 0;
+    TCHK(cudaMemcpyAsync(&nt, flag + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TCHK(cudaStreamSynchronize(s));
+    TCHK(dalloc(tbase, (long long)nt + 1));
+    k_task_base<<<grid_for((long long)n + 1, 256), 256, 0, s>>>(flag, key, cnt, n, R, *tbase);
+    TCHK(cudaGetLastError());
+    TCHK(cudaStreamSynchronize(s));
+#undef TCHK
+    cleanup();
+    *ntasks = nt;
+    return 0;
+}
 
 long long scan_scratch_ints(long long m) { return (m + kScanTile - 1) / kScanTile + 1; }
 

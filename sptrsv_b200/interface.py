@@ -182,8 +182,13 @@ class Plan:
     def handle(self):
         return self._h
 
-    def set_schedule(self, variant: int, rows_per_warp: int = 1, ir_max_iters: int = 2, block_warps: int = 8):
-        s = Schedule(variant, rows_per_warp, block_warps, ir_max_iters)
+    def set_schedule(self, variant: int, rows_per_warp: int = 1, ir_max_iters: int = 2, block_warps: int = 8,
+                     warps_per_sm: int = 0, backoff_ns: int = 0, band_levels: int = 64, cluster_rows: int = 4096):
+        s = Schedule(variant, rows_per_warp, block_warps, warps_per_sm, backoff_ns, ir_max_iters, band_levels,
+                     cluster_rows)
+        C.check(C.lib().sptrsv_plan_set_schedule(self._h, byref(s)))
+
+    def set_schedule_struct(self, s: Schedule):
         C.check(C.lib().sptrsv_plan_set_schedule(self._h, byref(s)))
 
     def schedule(self) -> Schedule:

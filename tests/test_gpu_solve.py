@@ -114,15 +114,21 @@ def test_plan_variants_fp64_and_ir(torch_cuda, name):
     plan = S.Plan(L, info)
     db = torch.from_numpy(b).cuda()
     dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
-    for var in (S._lib.VAR_SIMPLE, S._lib.VAR_ORDER, S._lib.VAR_MULTIROW):
-        for rpw in ((1,) if var == S._lib.VAR_MULTIROW else (1, 2, 8, 32)):
-            plan.set_schedule(var, rpw, ir_max_iters=2)
-            plan.solve_f64(db, dx)
-            S.sync_status()
-            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, (var, rpw)
-            plan.solve_ir(db, dx)
-            S.sync_status()
-            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", var, rpw)
+    scheds = [dict(variant=v, rows_per_warp=r) for v in (S._lib.VAR_SIMPLE, S._lib.VAR_ORDER)
+              for r in (1, 2, 8, 32)]
+    scheds += [dict(variant=S._lib.VAR_MULTIROW, rows_per_warp=1),
+               dict(variant=S._lib.VAR_MULTIROW, rows_per_warp=1, block_warps=4, warps_per_sm=16, backoff_ns=200)]
+    scheds += [dict(variant=S._lib.VAR_CLUSTER, rows_per_warp=r, band_levels=h, cluster_rows=bsz, block_warps=bw)
+               for (r, h, bsz, bw) in ((1, 64, 4096, 8), (2, 16, 1024, 4), (16, 4, 256, 2), (32, 1, 32, 16),
+                                       (4, 128, 8192, 16))]
+    for sc in scheds:
+        plan.set_schedule(ir_max_iters=2, **sc)
+        plan.solve_f64(db, dx)
+        S.sync_status()
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, sc
+        plan.solve_ir(db, dx)
+        S.sync_status()
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", sc)
     dr = torch.empty_like(dx)
     plan.residual(db, dx, dr)
     S.sync_status()
