@@ -249,6 +249,28 @@ int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, 
 int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, double* r,
                         int nrhs, cudaStream_t stream);
 
+/* --- Batched solves: many systems, one persistent launch ------------------ */
+/* nsys independent systems (device CSRs, e.g. from allocate_memory), system s
+ * with nrhs[s] right-hand sides (1..32), solved together: one analysis of
+ * their block-diagonal union, rows laid out in (level, right-hand-side
+ * class) order, one persistent launch per solve, replayable as a CUDA graph.
+ * Vectors are packed: system s owns the row-major n_s x nrhs[s] block that
+ * starts at element offsets[s] (sptrsv_batch_info).  The batch keeps its own
+ * copy of the matrices. */
+typedef struct sptrsv_batch_s* sptrsv_batch_t;
+int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_batch_t* out);
+int sptrsv_batch_destroy(sptrsv_batch_t batch);
+/* offsets[nsys+1] (may be NULL), total rows, levels of the union, packed length. */
+int sptrsv_batch_info(sptrsv_batch_t batch, long long* offsets, int* n_total, int* nlevs, long long* vec_len);
+int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int block_warps, int warps_per_sm, int backoff_ns,
+                              int ir_iters);
+/* b, x: DEVICE packed vectors; precision 64 plain FP64, 32 FP32 + FP64 refinement. */
+int sptrsv_batch_solve(sptrsv_batch_t batch, const double* b, double* x, int precision, cudaStream_t stream);
+/* Same solve captured once as a CUDA graph for these (b, x, precision) and
+ * replayed on `stream`; a different (b, x, precision) captures again. */
+int sptrsv_batch_solve_graph(sptrsv_batch_t batch, const double* b, double* x, int precision,
+                             cudaStream_t stream);
+
 /* --- Schedule selection: features, autotuner, learned selector ------------ */
 
 /* 12 cheap features of an analysed matrix: log2 n, log2 nnz, nnz/n,

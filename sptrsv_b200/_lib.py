@@ -102,6 +102,12 @@ _SIGS = {
     "sptrsv_solve_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "sptrsv_residual_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_batch_create": (c_int, [c_int, POINTER(SpMat), c_void_p, POINTER(c_void_p)]),
+    "sptrsv_batch_destroy": (c_int, [c_void_p]),
+    "sptrsv_batch_info": (c_int, [c_void_p, c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong)]),
+    "sptrsv_batch_set_schedule": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "sptrsv_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_batch_solve_graph": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_features": (c_int, [POINTER(SpMat), POINTER(AnalysisInfo), c_void_p]),
     "sptrsv_schedule_from_class": (c_int, [c_int, POINTER(Schedule)]),
     "sptrsv_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, POINTER(c_int)]),

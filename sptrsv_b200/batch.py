@@ -1,0 +1,50 @@
+"""Batched solves over the C ABI: many independent systems, each with its own
+number of right-hand sides, in one persistent launch (optionally replayed
+from a CUDA graph)."""
+from __future__ import annotations
+
+from ctypes import byref, c_int, c_longlong, c_void_p
+
+import numpy as np
+
+from . import _lib as C
+from ._lib import SpMat
+from .interface import _dev, _stream
+
+
+class Batch:
+    def __init__(self, mats: list[SpMat], nrhs):
+        arr = (SpMat * len(mats))(*mats)
+        k = np.ascontiguousarray(nrhs, dtype=np.int32)
+        assert k.shape[0] == len(mats)
+        h = c_void_p()
+        C.check(C.lib().sptrsv_batch_create(len(mats), arr, k.ctypes.data, byref(h)))
+        self._h = h
+        self.nsys = len(mats)
+        self.nrhs = k
+        off = np.zeros(self.nsys + 1, dtype=np.int64)
+        n, nl, vl = c_int(0), c_int(0), c_longlong(0)
+        C.check(C.lib().sptrsv_batch_info(h, off.ctypes.data, byref(n), byref(nl), byref(vl)))
+        self.offsets, self.n, self.nlevs, self.vec_len = off, n.value, nl.value, vl.value
+
+    def set_schedule(self, block_warps: int = 8, warps_per_sm: int = 0, backoff_ns: int = 0, ir_iters: int = 2):
+        C.check(C.lib().sptrsv_batch_set_schedule(self._h, block_warps, warps_per_sm, backoff_ns, ir_iters))
+
+    def solve(self, b, x, precision: int = 32, stream=None):
+        C.check(C.lib().sptrsv_batch_solve(self._h, _dev(b, "float64", self.vec_len), _dev(x, "float64", self.vec_len),
+                                           precision, _stream(stream)))
+
+    def solve_graph(self, b, x, precision: int = 32, stream=None):
+        C.check(C.lib().sptrsv_batch_solve_graph(self._h, _dev(b, "float64", self.vec_len),
+                                                 _dev(x, "float64", self.vec_len), precision, _stream(stream)))
+
+    def close(self):
+        if self._h:
+            C.lib().sptrsv_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -62,49 +62,50 @@ __global__ void k_validate(const int* __restrict__ rowptr, const int* __restrict
     }
 }
 
-// Persistent sync-free level computation.  Task t covers rows
-// [t*R, t*R+R) of the natural order with L = 32/R lanes per row.
+// Persistent sync-free level computation over natural-order chunks: warp
+// task t covers rows [32t, 32t+32) and computes them one after another, all
+// 32 lanes striding a row's columns.  Natural order is topological, so a
+// dependency inside the chunk was computed by this warp a moment ago and is
+// read from the warp's shared-memory ring; a dependency outside is polled
+// warp-convergently (level 0 = not yet written).  Row metadata of the whole
+// chunk is loaded up front, one row per lane.
 __global__ void __launch_bounds__(256) k_levels(const int* __restrict__ rowptr, const int* __restrict__ col, int n,
-                                                int L, int* level, int* nlevs, DevStatus* st,
-                                                unsigned long long budget)
+                                                int* level, int* nlevs, DevStatus* st, unsigned long long budget)
 {
+    __shared__ int ring[8][32];
     const int lane = threadIdx.x & 31;
-    const int R = 32 / L;
-    const int seg = lane / L, sl = lane & (L - 1);
-    // consecutive rows of one task may depend on each other: each row's lanes
-    // reduce and publish under their own mask before the warp converges
-    const unsigned smask = L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (seg * L));
+    int* my = ring[threadIdx.x >> 5];
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long ntasks = ((long long)n + R - 1) / R;
+    const long long ntasks = ((long long)n + 31) / 32;
     int my_max = 0;
     for (long long t = gw; t < ntasks; t += nw) {
-        long long r64 = t * R + seg;
-        bool act = r64 < n;
-        int r = (int)r64;
-        int m = 0;
-        bool fail = false;
-        if (act) {
-            int s = __ldg(rowptr + r), e = __ldg(rowptr + r + 1) - 1;
-            for (int p = s + sl; p < e; p += L) {
-                int c = __ldg(col + p);
-                int lv;
-                if (!wait_ready(level + c, lv, st, budget, r)) {
-                    fail = true;
-                    break;
-                }
-                m = max(m, lv);
+        const int r0 = (int)(t * 32), cnt = min(32, n - r0);
+        int ms = 0, me = 0;
+        if (lane < cnt) {
+            ms = __ldg(rowptr + r0 + lane);
+            me = __ldg(rowptr + r0 + lane + 1) - 1;
+        }
+        for (int j = 0; j < cnt; j++) {
+            const int s = __shfl_sync(0xffffffffu, ms, j), e = __shfl_sync(0xffffffffu, me, j);
+            int m = 0;
+            for (int p = s + lane; __any_sync(0xffffffffu, p < e); p += 32) {
+                const bool have = p < e;
+                const int c = have ? __ldg(col + p) : 0;
+                const bool local = have && c >= r0;
+                int lv = local ? my[c - r0] : 0;
+                if (!warp_wait<false, int>(have && !local, c, level, nullptr, lv, st, budget, 0u, r0 + j)) return;
+                if (have) m = max(m, lv);
             }
-        }
-        for (int o = L >> 1; o >= 1; o >>= 1) m = max(m, __shfl_down_sync(smask, m, o, L));
-        const bool seg_fail = __any_sync(smask, fail);
-        if (act && sl == 0 && !seg_fail) {
-            st_relaxed(level + r, m + 1);
+            m = __reduce_max_sync(0xffffffffu, m);
+            if (lane == 0) {
+                my[j] = m + 1;
+                st_relaxed(level + r0 + j, m + 1);
+            }
             my_max = max(my_max, m + 1);
+            __syncwarp();
         }
-        if (__any_sync(0xffffffffu, seg_fail)) return;
     }
-    for (int o = 16; o >= 1; o >>= 1) my_max = max(my_max, __shfl_down_sync(0xffffffffu, my_max, o));
     if (lane == 0 && my_max > 0) atomicMax(nlevs, my_max);
 }
 
@@ -169,14 +170,6 @@ __global__ void k_inverse(const int* __restrict__ perm, int n, int* __restrict__
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) inv[perm[k]] = k;
 }
 
-
-// Lanes per row of the level kernel.  The reference picks a tile of 1-32
-// lanes from nnz/n (aux_call_kernel_analysis_L_coop_groups, :216-239), which
-// puts consecutive rows of the natural order in one warp; consecutive rows
-// often depend on each other, and a producer and a waiting consumer in the
-// same warp make progress only when the scheduler switches between the
-// diverged paths.  One row per warp keeps dependent rows in different warps.
-int level_lanes(int, int) { return 32; }
 
 
 }  // namespace
@@ -262,10 +255,9 @@ int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode)
     // 1. levels
     int nlevs = 0;
     if (n > 0) {
-        int lanes = level_lanes(nnz, n);
-        long long rows_per_block = 8LL * (32 / lanes);
-        ACHK(launch_persistent(k_levels, 256, 0, (n + rows_per_block - 1) / rows_per_block, s, L->ia, L->ja, n,
-                               lanes, rec->d_levels, d_nlevs, c->d_status, wait_budget_ns()));
+        // one 32-row chunk per warp, 8 warps per block
+        ACHK(launch_persistent(k_levels, 256, 0, ((long long)n + 255) / 256, s, L->ia, L->ja, n, rec->d_levels,
+                               d_nlevs, c->d_status, wait_budget_ns()));
         ACHK(cudaMemcpyAsync(&nlevs, d_nlevs, sizeof(int), cudaMemcpyDeviceToHost, s));
         int st = sync_status(s);
         if (st) return fail(st);

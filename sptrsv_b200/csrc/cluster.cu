@@ -108,6 +108,8 @@ __global__ void k_cluster_fill(SptLayout lev, const int* __restrict__ lev_inv, S
         if (lane == 0) {
             clu.dg64[k] = lev.dg64[q];
             clu.dg32[k] = lev.dg32[q];
+            clu.di64[k] = lev.di64[q];
+            clu.di32[k] = lev.di32[q];
         }
     }
 }
@@ -136,10 +138,9 @@ __global__ void k_cluster_first_task(const int* __restrict__ cptr, int nclusters
 
 int build_order_tasks(sptrsv_plan_s* p, int R)
 {
-    if (p->ord_tasks && p->ord_R == R) return 0;
-    cudaFree(p->ord_tasks);
-    p->ord_tasks = nullptr;
-    p->ord_ntasks = 0;
+    int j = 0;
+    while ((1 << j) < R) j++;
+    if (p->ord_tasks[j]) return 0;
     int* key = nullptr;
     SPT_CUDA(dalloc(&key, p->n));
     if (p->n > 0) {
@@ -150,11 +151,9 @@ int build_order_tasks(sptrsv_plan_s* p, int R)
             return cuda_fail(e, "order tasks");
         }
     }
-    int rc = build_task_table(key, p->n, p->nlevs > 0 ? p->nlevs : 1, R, &p->ord_tasks, &p->ord_ntasks, 0);
+    int rc = build_task_table(key, p->n, p->nlevs > 0 ? p->nlevs : 1, R, &p->ord_tasks[j], &p->ord_ntasks[j], 0);
     cudaFree(key);
-    if (rc) return rc;
-    p->ord_R = R;
-    return 0;
+    return rc;
 }
 
 int build_cluster_tasks(sptrsv_plan_s* p, int R)
@@ -185,6 +184,8 @@ void layout_free(SptLayout& l)
     cudaFree(l.val32);
     cudaFree(l.dg64);
     cudaFree(l.dg32);
+    cudaFree(l.di64);
+    cudaFree(l.di32);
     l = SptLayout();
 }
 
@@ -197,6 +198,8 @@ int layout_alloc(SptLayout& l, int n, int m)
     SPT_CUDA(dalloc(&l.val32, m));
     SPT_CUDA(dalloc(&l.dg64, n));
     SPT_CUDA(dalloc(&l.dg32, n));
+    SPT_CUDA(dalloc(&l.di64, n));
+    SPT_CUDA(dalloc(&l.di32, n));
     return 0;
 }
 

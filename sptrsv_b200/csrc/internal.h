@@ -113,8 +113,10 @@ cudaError_t radix_sort_pairs(int* keys, int* vals, int* keys_tmp, int* vals_tmp,
 // Segment-aligned task table.  key[p] (p < n) is non-decreasing, in [0, K);
 // a segment is a run of equal keys.  Tasks are runs of at most R positions
 // inside one segment, so rows of one task never depend on each other when a
-// segment is (part of) a level.  *tbase gets ntasks+1 entries (allocated
-// here; tbase[ntasks] = n).  Returns 0 or an error code.
+// segment is (part of) a level.  R <= 0 takes R = 32 >> (key % 6) per
+// segment (keys that carry a lane class in their low base-6 digit).
+// *tbase gets ntasks+1 entries (allocated here; tbase[ntasks] = n).
+// Returns 0 or an error code.
 int build_task_table(const int* key, int n, int K, int R, int** tbase, int* ntasks, cudaStream_t s);
 
 // ---- analysis record -------------------------------------------------------

@@ -9,6 +9,7 @@
 //   val64[m]    f64     off-diagonal values
 //   val32[m]    f32     the same values rounded to FP32
 //   dg64[n], dg32[n]    diagonal per position
+//   di64[n], di32[n]    its reciprocal (the reference's piv = 1/diag)
 // The level layout (iorder sequence) is always built; it serves SIMPLE
 // (through inv[n], natural row -> position), ORDER, MULTIROW (with the
 // analysis warp map ibase/ivect) and the FP64 residual.  The cluster layout
@@ -28,6 +29,8 @@ struct SptLayout {
     float* val32 = nullptr;
     double* dg64 = nullptr;
     float* dg32 = nullptr;
+    double* di64 = nullptr;  // 1 / diagonal, rounded once in f64
+    float* di32 = nullptr;   // 1.0f / (float)diagonal
 };
 
 struct sptrsv_plan_s {
@@ -38,8 +41,8 @@ struct sptrsv_plan_s {
     int* levels = nullptr;       // 1-based level per row
     int* ibase = nullptr;        // multirow map
     int* ivect = nullptr;
-    int* ord_tasks = nullptr;    // level-aligned tasks over the level layout
-    int ord_ntasks = 0, ord_R = 0;
+    int* ord_tasks[6] = {};      // level-aligned tasks over the level layout, R = 1 << j rows
+    int ord_ntasks[6] = {};
     SptLayout clu;               // cluster order (built on demand)
     int* cptr = nullptr;
     int* clu_key = nullptr;      // per position: cluster * H + local level

@@ -85,14 +85,19 @@ int solve_reference(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b, d
         if (e) return e;
         SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(ntasks, kRefWarps), s, m, n, ntasks, lanes, tasks,
                                    (const int*)nullptr, b, x, (double*)nullptr, c->d_status, budget, 0u));
+    } else if (mode == ORDER) {
+        // one row per warp, in iorder (solve_csr_order.cu:83-149)
+        SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(n, kRefWarps), s, m, n, n, 32, (const int*)nullptr,
+                                   (const int*)nullptr, b, x, (double*)nullptr, c->d_status, budget, 0u));
     } else {
-        // SIMPLE walks the natural order: one row per warp by default, so that
-        // consecutive (often dependent) rows never share a warp
-        int L = lanes ? lanes : 32;
-        int ntasks = div_up(n, 32 / L);
-        SPT_CUDA(launch_persistent(kern, kRefBlock, 0, div_up(ntasks, kRefWarps), s, m, n, ntasks, L,
-                                   (const int*)nullptr, (const int*)nullptr, b, x, (double*)nullptr, c->d_status,
-                                   budget, 0u));
+        // SIMPLE (solve_csr_simple.cu:10-108) walks the natural order in
+        // chunks: the reference gives a block a run of rows and resolves
+        // dependencies inside the block through shared memory; here a warp
+        // takes 32 consecutive rows, solves them in sequence and reads
+        // in-chunk dependencies from its shared-memory ring
+        auto kc = k_sptrsv_chunk<NatMat, double, double, OUT_X>;
+        SPT_CUDA(launch_persistent(kc, kRefBlock, 0, div_up(div_up(n, 32), kRefWarps), s, m, n, 32, b, x,
+                                   (double*)nullptr, c->d_status, budget, 0u));
     }
     return ok();
 }
@@ -131,8 +136,11 @@ __global__ void k_plan_fill(const int* __restrict__ rowptr, const int* __restric
             l.val32[o + p - s] = (float)v;
         }
         if (lane == 0) {
-            l.dg64[k] = val[e];
-            l.dg32[k] = (float)val[e];
+            double d = val[e];
+            l.dg64[k] = d;
+            l.dg32[k] = (float)d;
+            l.di64[k] = 1.0 / d;
+            l.di32[k] = 1.0f / (float)d;
         }
     }
 }
@@ -142,7 +150,8 @@ void plan_free_arrays(sptrsv_plan_s* p)
     layout_free(p->lev);
     layout_free(p->clu);
     cudaFree(p->cptr); cudaFree(p->inv); cudaFree(p->levels); cudaFree(p->ibase); cudaFree(p->ivect);
-    cudaFree(p->ord_tasks); cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
+    for (int j = 0; j < 6; j++) cudaFree(p->ord_tasks[j]);
+    cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
     cudaFree(p->w32a); cudaFree(p->w32b); cudaFree(p->hb); cudaFree(p->hx);
 }
 
@@ -209,22 +218,24 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
     const int n = p->n;
     const int block = 32 * sc.block_warps;
     const int cap = sc.warps_per_sm > 0 ? (sc.warps_per_sm + sc.block_warps - 1) / sc.block_warps : 0;
-    auto layout_vals = [&](const SptLayout& l, const V*& val, const V*& dg) {
+    auto layout_vals = [&](const SptLayout& l, const V*& val, const V*& dg, const V*& di) {
         if (f32) {
             val = reinterpret_cast<const V*>(l.val32);
             dg = reinterpret_cast<const V*>(l.dg32);
+            di = reinterpret_cast<const V*>(l.di32);
         } else {
             val = reinterpret_cast<const V*>(l.val64);
             dg = reinterpret_cast<const V*>(l.dg64);
+            di = reinterpret_cast<const V*>(l.di64);
         }
     };
     if (sc.variant == SPTRSV_VAR_CLUSTER && nrhs == 1) {
         int e = build_cluster_layout(p, sc.band_levels, sc.cluster_rows);
         if (!e) e = build_cluster_tasks(p, sc.rows_per_warp);
         if (e) return e;
-        const V *val, *dg;
-        layout_vals(p->clu, val, dg);
-        PermMat<V> m{p->clu.ptr, p->clu.rowid, p->clu.col, val, dg, nullptr};
+        const V *val, *dg, *di;
+        layout_vals(p->clu, val, dg, di);
+        PermMat<V> m{p->clu.ptr, p->clu.rowid, p->clu.col, val, dg, di, nullptr};
         auto kern = k_sptrsv_cluster<V, T, BT, OUT>;
         size_t smem = sizeof(T) * (size_t)p->clu_B;
         SPT_CUDA(allow_smem(kern, smem));
@@ -233,18 +244,31 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
                                           32 / sc.rows_per_warp, b, x, x64, c->d_status, budget, backoff));
         return 0;
     }
-    const V *val, *dg;
-    layout_vals(p->lev, val, dg);
-    PermMat<V> m{p->lev.ptr, p->lev.rowid, p->lev.col, val, dg,
+    const V *val, *dg, *di;
+    layout_vals(p->lev, val, dg, di);
+    PermMat<V> m{p->lev.ptr, p->lev.rowid, p->lev.col, val, dg, di,
                  sc.variant == SPTRSV_VAR_SIMPLE ? p->inv : nullptr};
     const int wpb = sc.block_warps;
     if (nrhs > 1) {
-        int kp = 1;
+        // multi-RHS: level-aligned tasks of 32/kp rows over the level layout
+        PermMat<V> ml = m;
+        ml.seq = nullptr;
+        int kp = 1, j = 0;
         while (kp < nrhs) kp <<= 1;
-        int ntasks = div_up(n, 32 / kp);
+        int e = build_order_tasks(p, 32 / kp);
+        if (e) return e;
+        while ((1 << j) < 32 / kp) j++;
         auto kern = k_sptrsv_mrhs<PermMat<V>, T, BT, OUT>;
-        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(ntasks, wpb), cap, s, m, n, nrhs, kp, b, x, x64,
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->ord_ntasks[j], wpb), cap, s, ml,
+                                          p->ord_ntasks[j], (const int*)p->ord_tasks[j], nrhs, kp, b, x, x64,
                                           c->d_status, budget, backoff));
+        return 0;
+    }
+    if (sc.variant == SPTRSV_VAR_SIMPLE) {
+        // natural-order chunks of rows_per_warp rows, solved in sequence by a warp
+        auto kern = k_sptrsv_chunk<PermMat<V>, T, BT, OUT>;
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(div_up(n, sc.rows_per_warp), wpb), cap, s, m, n,
+                                          sc.rows_per_warp, b, x, x64, c->d_status, budget, backoff));
         return 0;
     }
     auto kern = k_sptrsv<PermMat<V>, T, BT, OUT>;
@@ -252,19 +276,15 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->n_warps, wpb), cap, s, m, n, p->n_warps, 0,
                                           (const int*)p->ibase, (const int*)p->ivect, b, x, x64, c->d_status, budget,
                                           backoff));
-    } else if (sc.variant == SPTRSV_VAR_ORDER) {
-        // level-aligned tasks: rows of one warp never depend on each other
+    } else {
+        // ORDER: level-aligned tasks, rows of one warp never depend on each other
+        int j = 0;
+        while ((1 << j) < sc.rows_per_warp) j++;
         int e = build_order_tasks(p, sc.rows_per_warp);
         if (e) return e;
-        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->ord_ntasks, wpb), cap, s, m, n, p->ord_ntasks,
-                                          32 / sc.rows_per_warp, (const int*)p->ord_tasks, (const int*)nullptr, b, x,
-                                          x64, c->d_status, budget, backoff));
-    } else {
-        int L = 32 / sc.rows_per_warp;
-        int ntasks = div_up(n, sc.rows_per_warp);
-        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(ntasks, wpb), cap, s, m, n, ntasks, L,
-                                          (const int*)nullptr, (const int*)nullptr, b, x, x64, c->d_status, budget,
-                                          backoff));
+        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->ord_ntasks[j], wpb), cap, s, m, n,
+                                          p->ord_ntasks[j], 32 / sc.rows_per_warp, (const int*)p->ord_tasks[j],
+                                          (const int*)nullptr, b, x, x64, c->d_status, budget, backoff));
     }
     return 0;
 }
@@ -272,7 +292,7 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
 int plan_residual(sptrsv_plan_s* p, const double* b, const double* x, float* r32, double* r64, int nrhs,
                   cudaStream_t s)
 {
-    PermMat<double> m{p->lev.ptr, p->lev.rowid, p->lev.col, p->lev.val64, p->lev.dg64, nullptr};
+    PermMat<double> m{p->lev.ptr, p->lev.rowid, p->lev.col, p->lev.val64, p->lev.dg64, p->lev.di64, nullptr};
     const int n = p->n;
     if (nrhs > 1) {
         int kp = 1;

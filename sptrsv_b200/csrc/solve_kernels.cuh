@@ -51,6 +51,8 @@ struct NatMat {
         return q;
     }
     __device__ __forceinline__ double diag(const RowRef& q) const { return __ldg(val + q.d); }
+    // piv = 1 / diag as the reference computes it (solve_csr_order.cu:239)
+    __device__ __forceinline__ double inv(const RowRef& q) const { return 1.0 / __ldg(val + q.d); }
     __device__ __forceinline__ int c(int p) const { return __ldg(col + p); }
     __device__ __forceinline__ double v(int p) const { return __ldg(val + p); }
 };
@@ -62,8 +64,10 @@ struct PermMat {
     const int* __restrict__ col;    // off-diagonal columns (original indices)
     const VT* __restrict__ val;     // off-diagonal values
     const VT* __restrict__ dg;      // [n] diagonal per position
+    const VT* __restrict__ di;      // [n] 1 / diagonal (rounded once, as 1/diag in VT)
     const int* __restrict__ seq;    // null: layout order; else natural -> position
     typedef VT V;
+    __device__ __forceinline__ VT inv(const RowRef& q) const { return __ldg(di + q.d); }
     __device__ __forceinline__ RowRef row(int pos) const
     {
         RowRef q;
@@ -95,6 +99,96 @@ __device__ __forceinline__ unsigned segment_mask(int L, int seg)
     return L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (seg * L));
 }
 
+// Per-lane state of one task.  Loaded one task ahead (software pipelining):
+// the next task's row metadata, reciprocal diagonal, right-hand side and
+// first element are in flight while the current task waits on its
+// dependencies, so a warp that moves on only pays for the wait itself.
+template <typename T>
+struct Slot {
+    int base, cnt, L;  // warp-uniform: first position, rows, lanes per row (0: diagonal-only rows)
+    bool act;          // this lane's segment holds a row
+    RowRef q;
+    T piv;             // 1/diag (diagonal itself when L == 0)
+    T acc;             // b for the segment's first lane, else 0
+    int c0;            // first element of this lane (if q.s + sl < q.e)
+    T v0;
+};
+
+template <class M, typename T, typename BT>
+__device__ __forceinline__ void load_slot(Slot<T>& s, const M& m, int base, int cnt, int L, int lane,
+                                          const BT* __restrict__ b)
+{
+    s.base = base;
+    s.cnt = cnt;
+    s.L = L;
+    if (L == 0) {
+        s.act = lane < cnt;
+        if (s.act) {
+            s.q = m.row(base + lane);
+            s.piv = (T)m.diag(s.q);
+            s.acc = (T)b[s.q.r];
+        }
+        return;
+    }
+    const int seg = lane / L, sl = lane & (L - 1);
+    s.act = seg < cnt;
+    if (s.act) {
+        s.q = m.row(base + seg);
+        s.piv = (T)m.inv(s.q);
+        s.acc = sl == 0 ? (T)b[s.q.r] : (T)0;
+        const int p = s.q.s + sl;
+        if (p < s.q.e) {
+            s.c0 = m.c(p);
+            s.v0 = (T)m.v(p);
+        }
+    }
+}
+
+// Runs one task: each lane takes its row's elements in rounds (lane sl of a
+// row takes elements sl, sl+L, ...), the warp waits for a round's
+// dependencies together, then rows reduce under their segment mask and
+// publish.  Rows of one task are independent (tasks are level-aligned), so
+// a warp-wide wait cannot deadlock.  Returns true (warp-uniform) on failure.
+template <bool SMEM, class M, typename T, int OUT>
+__device__ __forceinline__ bool run_slot(const Slot<T>& s, const M& m, int lane, T* x, double* x64, volatile T* xs,
+                                         int cs, DevStatus* st, unsigned long long budget, unsigned backoff)
+{
+    if (s.L == 0) {  // diagonal-only rows: x = b / diag (solve_csr_multirow.cu:56-59)
+        if (s.act) {
+            T v = publishable(s.acc / s.piv);
+            if (SMEM) xs[s.base + lane - cs] = v;
+            publish<T, OUT>(x, x64, s.q.r, v);
+        }
+        return false;
+    }
+    const int L = s.L, seg = lane / L, sl = lane & (L - 1);
+    const unsigned smask = segment_mask(L, seg);
+    T acc = s.acc;
+    const int mine = s.act ? max(0, (s.q.e - s.q.s - sl + L - 1) / L) : 0;
+    const int rounds = __reduce_max_sync(0xffffffffu, mine);
+    int p = s.q.s + sl;
+    int c = s.c0;
+    T v = s.v0;
+    for (int j = 0; j < rounds; j++) {
+        const bool have = j < mine;
+        if (have && j > 0) {
+            c = m.c(p);
+            v = (T)m.v(p);
+        }
+        T xv = 0;
+        if (!warp_wait<SMEM, T>(have, c, x, xs, xv, st, budget, backoff, s.q.r)) return true;
+        if (have) acc -= v * xv;
+        p += L;
+    }
+    for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
+    if (s.act && sl == 0) {
+        T val = publishable(acc * s.piv);
+        if (SMEM) xs[s.base + seg - cs] = val;
+        publish<T, OUT>(x, x64, s.q.r, val);
+    }
+    return false;
+}
+
 // Single right-hand side.  Task t: `lanes` lanes per row, 32/lanes rows.
 // No table: task t covers positions [t*R, t*R+R) with fixed lanes.
 // Table: task t covers [task_base[t], task_base[t+1]) with task_lanes[t]
@@ -110,7 +204,7 @@ __global__ void __launch_bounds__(512) k_sptrsv(M m, int npos, int ntasks, int f
     const int lane = threadIdx.x & 31;
     const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-    for (int t = gw; t < ntasks; t += nw) {
+    auto load = [&](Slot<T>& s, int t) {
         int L, base, cnt;
         if (task_base) {
             base = __ldg(task_base + t);
@@ -121,43 +215,17 @@ __global__ void __launch_bounds__(512) k_sptrsv(M m, int npos, int ntasks, int f
             base = t * (32 / L);
             cnt = min(32 / L, npos - base);
         }
-        if (L == 0) {  // diagonal-only rows: x = b / diag
-            if (lane < cnt) {
-                RowRef q = m.row(base + lane);
-                T v = (T)b[q.r] / (T)m.diag(q);
-                publish<T, OUT>(x, x64, q.r, v);
-            }
-            continue;
-        }
-        // Rows of one task may depend on each other (fixed lanes over level or
-        // natural order), so each row's lanes reduce and publish on their own
-        // (segment mask); the warp converges only after every row published.
-        const int seg = lane / L, sl = lane & (L - 1);
-        const unsigned smask = segment_mask(L, seg);
-        const bool act = seg < cnt;
-        T acc = 0;
-        bool fail = false;
-        RowRef q;
-        T piv = 0;
-        if (act) {
-            q = m.row(base + seg);
-            piv = (T)1 / (T)m.diag(q);
-            if (sl == 0) acc = (T)b[q.r];
-            for (int p = q.s + sl; p < q.e; p += L) {
-                int c = m.c(p);
-                T v = (T)m.v(p);
-                T xv;
-                if (!wait_ready(x + c, xv, st, budget, q.r, backoff)) {
-                    fail = true;
-                    break;
-                }
-                acc -= v * xv;
-            }
-        }
-        for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
-        const bool seg_fail = __any_sync(smask, fail);
-        if (act && sl == 0 && !seg_fail) publish<T, OUT>(x, x64, q.r, acc * piv);
-        if (__any_sync(0xffffffffu, seg_fail)) return;
+        load_slot(s, m, base, cnt, L, lane, b);
+    };
+    int t = gw;
+    Slot<T> cur, nxt;
+    if (t < ntasks) load(cur, t);
+    while (t < ntasks) {
+        const int tn = t + nw;
+        if (tn < ntasks) load(nxt, tn);
+        if (run_slot<false, M, T, OUT>(cur, m, lane, x, x64, nullptr, 0, st, budget, backoff)) return;
+        cur = nxt;
+        t = tn;
     }
 }
 
@@ -178,50 +246,28 @@ __global__ void __launch_bounds__(512) k_sptrsv_cluster(PermMat<V> m, const int*
     volatile T* xs = reinterpret_cast<volatile T*>(smem_raw);
     __shared__ int abort_flag;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-    const int seg = lane / L, sl = lane & (L - 1);
-    const unsigned smask = segment_mask(L, seg);
     for (int c = blockIdx.x; c < nclusters; c += gridDim.x) {
         const int cs = __ldg(cptr + c), cn = __ldg(cptr + c + 1) - cs;
         for (int i = threadIdx.x; i < cn; i += blockDim.x) xs[i] = sentinel_value<T>();
         if (threadIdx.x == 0) abort_flag = 0;
         __syncthreads();
-        const int t0 = __ldg(ctask + c), t1 = __ldg(ctask + c + 1);
-        for (int t = t0 + wib; t < t1; t += nwb) {
-            const int tb = __ldg(tbase + t), tcnt = __ldg(tbase + t + 1) - tb;
-            const int loc = tb - cs + seg;
-            const bool act = seg < tcnt;
-            T acc = 0;
-            bool fail = false;
-            RowRef q;
-            T piv = 0;
-            if (act) {
-                q = m.row(cs + loc);
-                piv = (T)1 / (T)m.diag(q);
-                if (sl == 0) acc = (T)b[q.r];
-                for (int p = q.s + sl; p < q.e; p += L) {
-                    int cc = m.c(p);
-                    T v = (T)m.v(p);
-                    T xv;
-                    bool okw = cc < 0 ? wait_ready_smem(xs + (~cc), xv, st, budget, q.r)
-                                      : wait_ready(x + cc, xv, st, budget, q.r, backoff);
-                    if (!okw) {
-                        fail = true;
-                        break;
-                    }
-                    acc -= v * xv;
-                }
-            }
-            for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
-            const bool seg_fail = __any_sync(smask, fail);
-            if (act && sl == 0 && !seg_fail) {
-                T val = publishable(acc * piv);
-                xs[loc] = val;
-                publish<T, OUT>(x, x64, q.r, val);
-            }
-            if (__any_sync(0xffffffffu, seg_fail)) {
+        const int t1 = __ldg(ctask + c + 1);
+        auto load = [&](Slot<T>& s, int t) {
+            const int tb = __ldg(tbase + t);
+            load_slot(s, m, tb, __ldg(tbase + t + 1) - tb, L, lane, b);
+        };
+        int t = __ldg(ctask + c) + wib;
+        Slot<T> cur, nxt;
+        if (t < t1) load(cur, t);
+        while (t < t1) {
+            const int tn = t + nwb;
+            if (tn < t1) load(nxt, tn);
+            if (run_slot<true, PermMat<V>, T, OUT>(cur, m, lane, x, x64, xs, cs, st, budget, backoff)) {
                 if (lane == 0) abort_flag = 1;
                 break;
             }
+            cur = nxt;
+            t = tn;
         }
         __syncthreads();
         if (abort_flag) return;
@@ -229,39 +275,115 @@ __global__ void __launch_bounds__(512) k_sptrsv_cluster(PermMat<V> m, const int*
 }
 
 // nrhs right-hand sides (row-major n x K).  kp = power of two >= K lanes per
-// row, 32/kp rows per task; lane k of a row owns right-hand side k.
+// row; level-aligned task t covers positions [tbase[t], tbase[t+1]) (at
+// most 32/kp rows); lane k of a row owns right-hand side k and walks all of
+// the row's elements, the warp waiting for each round together.
 template <class M, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(512) k_sptrsv_mrhs(M m, int npos, int K, int kp, const BT* __restrict__ b, T* x,
-                                                     double* x64, DevStatus* st, unsigned long long budget,
-                                                     unsigned backoff)
+__global__ void __launch_bounds__(512) k_sptrsv_mrhs(M m, int ntasks, const int* __restrict__ tbase, int K, int kp,
+                                                     const BT* __restrict__ b, T* x, double* x64, DevStatus* st,
+                                                     unsigned long long budget, unsigned backoff)
 {
     const int lane = threadIdx.x & 31;
-    const int R = 32 / kp;
     const int seg = lane / kp, k = lane & (kp - 1);
     const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-    const int ntasks = (npos + R - 1) / R;
     for (int t = gw; t < ntasks; t += nw) {
-        int pos = t * R + seg;
-        bool act = pos < npos && k < K;
-        bool fail = false;
+        const int base = __ldg(tbase + t), cnt = __ldg(tbase + t + 1) - base;
+        const bool act = seg < cnt && k < K;
+        RowRef q;
+        T piv = 0, acc = 0;
+        int len = 0;
         if (act) {
-            RowRef q = m.row(pos);
-            T piv = (T)1 / (T)m.diag(q);
-            T acc = (T)b[(size_t)q.r * K + k];
-            for (int p = q.s; p < q.e; p++) {
-                int c = m.c(p);
-                T v = (T)m.v(p);
-                T xv;
-                if (!wait_ready(x + (size_t)c * K + k, xv, st, budget, q.r, backoff)) {
-                    fail = true;
-                    break;
-                }
-                acc -= v * xv;
-            }
-            if (!fail) publish<T, OUT>(x, x64, (size_t)q.r * K + k, acc * piv);
+            q = m.row(base + seg);
+            piv = (T)m.inv(q);
+            acc = (T)b[(size_t)q.r * K + k];
+            len = q.e - q.s;
         }
-        if (__any_sync(0xffffffffu, fail)) return;
+        const int rounds = __reduce_max_sync(0xffffffffu, len);
+        for (int j = 0; j < rounds; j++) {
+            const bool have = j < len;
+            int c = 0;
+            T v = 0, xv = 0;
+            if (have) {
+                c = m.c(q.s + j);
+                v = (T)m.v(q.s + j);
+            }
+            if (!warp_wait<false, T>(have, (int)((size_t)c * K + k), x, nullptr, xv, st, budget, backoff,
+                                     act ? q.r : -1))
+                return;
+            if (have) acc -= v * xv;
+        }
+        if (act) publish<T, OUT>(x, x64, (size_t)q.r * K + k, acc * piv);
+    }
+}
+
+// Natural-order chunks (the plan's SIMPLE schedule): warp task t covers the
+// natural rows [t*R, t*R+R) and solves them one after another with all 32
+// lanes striding each row's elements.  A dependency inside the chunk was
+// solved by this warp a moment ago and is read from the warp's shared-memory
+// ring without waiting; others are polled warp-convergently.  The next row's
+// metadata and first elements are loaded while the current row waits.
+template <class M, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(512) k_sptrsv_chunk(M m, int n, int R, const BT* __restrict__ b, T* x, double* x64,
+                                                      DevStatus* st, unsigned long long budget, unsigned backoff)
+{
+    __shared__ T ring[16][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T* my = ring[wib];
+    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    const int ntasks = (n + R - 1) / R;
+    for (int t = gw; t < ntasks; t += nw) {
+        const int r0 = t * R, cnt = min(R, n - r0);
+        // row j of the chunk: metadata in lane j (cnt <= 32)
+        RowRef mq;
+        T mpiv = 0, mb = 0;
+        if (lane < cnt) {
+            mq = m.row(r0 + lane);
+            mpiv = (T)m.inv(mq);
+            mb = (T)b[mq.r];
+        }
+        int ns = __shfl_sync(0xffffffffu, mq.s, 0), ne = __shfl_sync(0xffffffffu, mq.e, 0);
+        int nc = 0;
+        T nv = 0;
+        if (ns + lane < ne) {
+            nc = m.c(ns + lane);
+            nv = (T)m.v(ns + lane);
+        }
+        for (int j = 0; j < cnt; j++) {
+            const int s = ns, e = ne;
+            int c = nc;
+            T v = nv;
+            const T piv = __shfl_sync(0xffffffffu, mpiv, j);
+            const T bj = __shfl_sync(0xffffffffu, mb, j);
+            T acc = lane == 0 ? bj : (T)0;
+            if (j + 1 < cnt) {  // prefetch the next row's first elements
+                ns = __shfl_sync(0xffffffffu, mq.s, j + 1);
+                ne = __shfl_sync(0xffffffffu, mq.e, j + 1);
+                if (ns + lane < ne) {
+                    nc = m.c(ns + lane);
+                    nv = (T)m.v(ns + lane);
+                }
+            }
+            for (int p = s + lane, first = 1; __any_sync(0xffffffffu, p < e); p += 32, first = 0) {
+                const bool have = p < e;
+                if (have && !first) {
+                    c = m.c(p);
+                    v = (T)m.v(p);
+                }
+                const bool local = have && c >= r0;
+                T xv = local ? my[c - r0] : (T)0;
+                if (!warp_wait<false, T>(have && !local, c, x, nullptr, xv, st, budget, backoff, r0 + j)) return;
+                if (have) acc -= v * xv;
+            }
+            for (int o = 16; o >= 1; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                T val = publishable(acc * piv);
+                my[j] = val;
+                publish<T, OUT>(x, x64, (size_t)(r0 + j), val);
+            }
+            __syncwarp();
+        }
     }
 }
 

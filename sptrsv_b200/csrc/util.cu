@@ -217,11 +217,14 @@ __global__ void k_seg_count(const int* __restrict__ key, int n, int* __restrict_
     }
 }
 
+// rows per task of a segment: R, or 32 >> (key % 6) when R <= 0
+__device__ __forceinline__ int task_rows(int R, int key) { return R > 0 ? R : (32 >> (key % 6)); }
+
 __global__ void k_task_flags(const int* __restrict__ key, const int* __restrict__ seg_ptr, int n, int R,
                              int* __restrict__ flag)
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x)
-        flag[p] = p < n ? ((p - seg_ptr[key[p]]) % R == 0) : 0;
+        flag[p] = p < n ? ((p - seg_ptr[key[p]]) % task_rows(R, key[p]) == 0) : 0;
 }
 
 __global__ void k_task_base(const int* __restrict__ flag_scan, const int* __restrict__ key,
@@ -229,7 +232,7 @@ __global__ void k_task_base(const int* __restrict__ flag_scan, const int* __rest
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x) {
         if (p == n) tbase[flag_scan[n]] = n;
-        else if ((p - seg_ptr[key[p]]) % R == 0) tbase[flag_scan[p]] = p;
+        else if ((p - seg_ptr[key[p]]) % task_rows(R, key[p]) == 0) tbase[flag_scan[p]] = p;
     }
 }
 

@@ -89,6 +89,23 @@ def from_arrays(rowptr, colidx, val) -> HostCsr:
                    np.ascontiguousarray(val, np.float64))
 
 
+def batch_config(nsys: int = 512, seed: int = 3, n_lo: int = 1000, n_hi: int = 200_000, bw_lo: int = 16,
+                 bw_hi: int = 4096, off_lo: int = 4, off_hi: int = 16, k_max: int = 32):
+    """Batched configuration: nsys banded systems with n log-uniform in
+    [n_lo, n_hi], bandwidth log-uniform in [bw_lo, bw_hi], off_lo..off_hi
+    off-diagonals per row, k ~ U{1..k_max} right-hand sides each.
+    Returns (list of HostCsr, list of nrhs, list of x_true (row-major n x k))."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), nsys)).astype(np.int64)
+    bws = np.exp(rng.uniform(np.log(bw_lo), np.log(bw_hi), nsys)).astype(np.int64)
+    ks = rng.integers(1, k_max + 1, nsys)
+    mats, xs = [], []
+    for s in range(nsys):
+        mats.append(banded(int(ns[s]), int(bws[s]), off_lo, off_hi, seed=seed * 1_000_003 + s))
+        xs.append(vector(int(ns[s]) * int(ks[s]), "uniform", seed=seed * 2_000_003 + s))
+    return mats, [int(k) for k in ks], xs
+
+
 # The benchmark configurations (square lower-triangular, see the header).
 def config(name: str, scale: float = 1.0):
     """(matrix, x_true, nrhs) for a named configuration.
