@@ -249,6 +249,24 @@ int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, 
 int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, double* r,
                         int nrhs, cudaStream_t stream);
 
+/* --- A solve that allocates nothing --------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they solve — code whose device heap is owned by a pool or an
+ * arena, or that must not call cudaMalloc after start-up.  The caller passes
+ * the device CSR (diagonal last), b and x (DEVICE, n values); no analysis or
+ * plan is needed.  FP32 solve in natural-order chunks, then ir_iters
+ * refinement steps (FP64 residual, FP32 correction, x += d in FP64).
+ * Scratch lives in a fixed file-scope device array (two FP32 vectors of
+ * SPTRSV_NOALLOC_MAX_ROWS and a status word; about 8 MiB on every GPU that
+ * loads the library, kept until exit): n above SPTRSV_NOALLOC_MAX_ROWS is
+ * rejected with SPTRSV_ERR_UNSUPPORTED.  The first call on a device looks up
+ * the array's device address (make that first call before any stream
+ * capture).  All calls share the array: calls that overlap on the GPU race.
+ * Waits for `stream` and returns 0 or a negative SPTRSV_ERR_* code. */
+#define SPTRSV_NOALLOC_MAX_ROWS (1 << 20)
+int sptrsv_solve_ir_noalloc(const sp_mat_t* gpu_L, const double* b, double* x, int ir_iters,
+                            cudaStream_t stream);
+
 /* --- Batched solves: many systems, one persistent launch ------------------ */
 /* nsys independent systems (device CSRs, e.g. from allocate_memory), system s
  * with nrhs[s] right-hand sides (1..32), solved together: one analysis of

@@ -102,6 +102,7 @@ _SIGS = {
     "sptrsv_solve_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "sptrsv_residual_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_solve_ir_noalloc": (c_int, [POINTER(SpMat), c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_batch_create": (c_int, [c_int, POINTER(SpMat), c_void_p, POINTER(c_void_p)]),
     "sptrsv_batch_destroy": (c_int, [c_void_p]),
     "sptrsv_batch_info": (c_int, [c_void_p, c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong)]),
