@@ -4,18 +4,24 @@
 Default workload: the 2D 5-point lower triangle on a 2048x2048 grid
 (n = 4,194,304, nnz = 12,578,816, 4095 levels), one right-hand side.
 
-  value      solves/s of the tuned FP32 + FP64-refinement solve, b and x
-             resident in HBM, CUDA events around each step, L2 flushed
-             (256 MiB write) before every step.
-  e2e        the same solve through the C ABI host-buffer entry point
-             (sptrsv_solve_host): pinned host b in, host x out, both copies
-             inside the timed region.
-  roofline   the dominant kernel (the FP32 sync-free solve launch):
-             algorithmic bytes per launch / its CUDA-event time, against the
-             measured HBM copy bandwidth.
-  cpu_baseline  serial FP64 forward substitution (the CPU oracle) on one
-             host core, a bounded sample of the same workload.
+  value         solves/s of the tuned solver (schedule from the learned
+                selector when its weights are present, else the exhaustive
+                autotuner; precision mode — plain FP64, or FP32 solves with
+                FP64 refinement at the calibrated step count — whichever is
+                faster), b and x resident in HBM, CUDA events around each
+                step, L2 flushed (256 MiB write) before every step.
+  fp32_refine   the tuned FP32 + FP64-refinement solve, reported beside it.
   plain_fp64    the drop-in FP64 path (csr_L_solve_multirow) on the same GPU.
+  e2e           the tuned solve through the C ABI host-buffer entry point
+                (sptrsv_solve_host): pinned host b in, host x out, both copies
+                inside the timed region.
+  roofline      the dominant kernel: algorithmic bytes per launch / its
+                CUDA-event time, against the measured HBM copy bandwidth.
+  cpu_baseline  serial FP64 forward substitution (the CPU oracle) on one host
+                core, a bounded sample of the same workload.
+  reference_kernels  the reference's own solvers built from its sources for
+                sm_100a (oracle/_ref), FP64, same matrix, run in a child
+                process with a time limit.
 
 --impl reference times the reference algorithm on the host cores instead:
 the reference ships no CPU solver, so this is the CPU oracle's
@@ -47,6 +53,8 @@ CONFIG_NAMES = {
     "c2": "Zipf(1.5) DAG n=2000000 (<=256 off-diagonals), 1 RHS",
     "c2k16": "Zipf(1.5) DAG n=2000000 (<=256 off-diagonals), 16 RHS",
 }
+TOL = 1e-12
+SELECTOR_WEIGHTS = ROOT / "sptrsv_b200" / "selector_weights.npz"
 
 
 def algorithmic_bytes(n: int, nnz: int, k: int) -> int:
@@ -56,11 +64,10 @@ def algorithmic_bytes(n: int, nnz: int, k: int) -> int:
 
 
 def f32_launch_bytes(n: int, nnz: int, k: int) -> int:
-    """Algorithmic bytes of one FP32 sync-free solve launch over the plan
-    layout: ptr, rowid, FP32 diagonal, int32 col + FP32 value per
-    off-diagonal, f64 b read, f32 x written."""
-    nnz_off = nnz - n
-    return 4 * (n + 1) + 4 * n + 4 * n + 8 * nnz_off + 8 * n * k + 4 * n * k
+    """Algorithmic bytes of one FP32 solve launch over a plan layout: ptr,
+    rowid, FP32 reciprocal diagonal, int32 col + FP32 value per off-diagonal,
+    f64 b read, f32 x written."""
+    return 4 * (n + 1) + 4 * n + 4 * n + 8 * (nnz - n) + 8 * n * k + 4 * n * k
 
 
 def measured_peak():
@@ -227,6 +234,66 @@ def cpu_baseline_sample(m, b, k, budget_s=10.0):
             "sample": f"{reps} serial FP64 forward substitutions of the full workload ({t_total:.1f} s)"}
 
 
+def reference_kernels(cfg: str, timeout_s: int = 240):
+    """The reference's solvers (oracle/_ref, built from its sources) on the same
+    matrix, in a child process so that a stuck reference kernel cannot take the
+    benchmark down; returns {solver: {"ms": median, "err": rel err}} or None."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    code = (
+        "import sys, json; sys.path.insert(0, %r)\n"
+        "from oracle import oracle as O\nfrom sptrsv_b200 import gen\n"
+        "m, xt, k = gen.config(%r)\nb = m.matvec(xt, k)\nref = O.solve(m.rowptr, m.colidx, m.val, b)\n"
+        "O.ref_lib().ref_set_watchdog_seconds(60.0)\nout = {}\n"
+        "for v, name in ((2, 'multirow'), (1, 'order'), (0, 'simple')):\n"
+        "    x, ms = O.ref_solve(v, m.rowptr, m.colidx, m.val, b, reps=5)\n"
+        "    out[name] = {'ms': ms, 'rel_err': O.rel_err(x, ref)}\n"
+        "    print(json.dumps(out), flush=True)\n" % (str(ROOT), cfg))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired as e:
+        out = (e.stdout or b"").decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
+        lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+        return dict(json.loads(lines[-1]), note="timed out") if lines else {"note": "timed out"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if not lines:
+        return {"note": f"failed rc={r.returncode}: {r.stderr.strip()[-200:]}"}
+    return json.loads(lines[-1])
+
+
+def chain_hop_us(torch, S, SEL, n=100_000):
+    """Per-dependency latency on a bidiagonal chain (one row per level): the
+    L2 hop (level-ordered warps, dependency in another SM's row) and the
+    shared-memory hop (cluster schedule, dependency in the same CTA)."""
+    from sptrsv_b200 import gen
+
+    rp = np.concatenate([[0, 1], 1 + 2 * np.arange(1, n)])
+    ci = np.concatenate([[0]] + [[i - 1, i] for i in range(1, n)])
+    va = np.ones(ci.shape[0])
+    va[rp[1:] - 1] = 2.0
+    m = gen.from_arrays(rp, ci, va)
+    L = S.allocate_memory(m.rowptr, m.colidx, m.val, n)
+    info = S.AnalysisInfo()
+    info.mode = S.ALL
+    S.run_analysis(info, L)
+    plan = S.Plan(L, info)
+    b = torch.ones(n, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    out = {}
+    for name, sc in (("l2_hop_us", dict(variant=S._lib.VAR_MULTIROW, warps_per_sm=8)),
+                     ("smem_hop_us", dict(variant=S._lib.VAR_CLUSTER, rows_per_warp=32, band_levels=4096,
+                                          cluster_rows=4096, block_warps=8))):
+        plan.set_schedule(**sc)
+        t = statistics.median(event_time_steps(torch, lambda: plan.solve_f64(b, x), 3, 1))
+        out[name] = 1e3 * t / n
+    S.sync_status()
+    plan.close()
+    S.free_device_analysis(L, info)
+    return out
+
+
 def load_traffic(kernel_key: str):
     p = ROOT / "profiles" / "ncu_traffic.json"
     if p.exists():
@@ -243,6 +310,7 @@ def run_ours(args, rank, world, local, dist):
     import sptrsv_b200 as S
     from oracle import oracle as O
     from sptrsv_b200 import gen
+    from sptrsv_b200 import select as SEL
 
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
@@ -267,91 +335,141 @@ def run_ours(args, rank, world, local, dist):
     def flush():
         flush_buf.fill_(1)
 
-    # schedule: short sweep of the FP32 solve over the variants (autotuned pick)
-    cands = [(S._lib.VAR_MULTIROW, 1)] + [(v, r) for v in (S._lib.VAR_ORDER, S._lib.VAR_SIMPLE)
-                                           for r in (1, 2, 4, 8, 16, 32)]
-    best = None
-    for var, rpw in cands:
-        plan.set_schedule(var, rpw, ir_max_iters=2)
-        ts = event_time_steps(torch, lambda: plan.solve_f32(db, dx32, k), 3, 1, flush, stream)
-        t = statistics.median(ts)
-        if best is None or t < best[0]:
-            best = (t, var, rpw)
-    plan.set_schedule(best[1], best[2], ir_max_iters=2)
-    S.sync_status()
+    # --- schedule: learned selector when trained, exhaustive autotuner beside it
+    t0 = time.perf_counter()
+    cls64, times64 = SEL.autotune(plan, db, dx, k, 64, reps=3)
+    cls32, times32 = SEL.autotune(plan, db, dx, k, 32, reps=3)
+    tune_s = time.perf_counter() - t0
+    learned = None
+    if SELECTOR_WEIGHTS.exists():
+        net = SEL.Mlp.load(SELECTOR_WEIGHTS)
+        f = SEL.features(L, info)
+        c = net.predict_class(f)
+        learned = {"class": c, "name": SEL.class_name(c), "time_over_best_fp64": float(times64[c] / times64[cls64])}
+        net.close()
+    sel64 = learned["class"] if learned else cls64
+    sel32 = learned["class"] if learned else cls32
+    plan.set_schedule_struct(SEL.schedule_from_class(sel32))
+    ir_iters, ir_est = plan.calibrate_ir(db, dx, k, tol=1e-13, max_iters=4)
 
-    # correctness of the timed paths against the FP64 oracle
+    def set_mode(mode):
+        s = SEL.schedule_from_class(sel64 if mode == 64 else sel32)
+        s.ir_max_iters = ir_iters
+        plan.set_schedule_struct(s)
+
+    def solve(mode):
+        return (lambda: plan.solve_f64(db, dx, k)) if mode == 64 else (lambda: plan.solve_ir(db, dx, k))
+
+    # pick the precision mode by a short measurement
+    mode_ms = {}
+    for mode in (64, 32):
+        set_mode(mode)
+        mode_ms[mode] = statistics.median(event_time_steps(torch, solve(mode), 5, 1, flush, stream))
+    mode = 64 if mode_ms[64] <= mode_ms[32] else 32
     ref = O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k)
-    plan.solve_ir(db, dx, k)
-    S.sync_status()
-    err_ir = O.rel_err(dx.cpu().numpy(), ref)
-    plan.solve_f64(db, dx, k)
-    S.sync_status()
-    err_f64 = O.rel_err(dx.cpu().numpy(), ref)
+    errs = {}
+    for md in (64, 32):
+        set_mode(md)
+        solve(md)()
+        S.sync_status()
+        errs[md] = O.rel_err(dx.cpu().numpy(), ref)
+    set_mode(mode)
 
-    # timed: FP32 + FP64 refinement, device-resident
-    sampler = ClockSampler(local) if rank == 0 or world > 1 else None
+    # --- timed: the tuned solve, device-resident
+    sampler = ClockSampler(local)
     barrier(dist)
     torch.cuda.synchronize()
-    if sampler:
-        sampler.start()
-    ts = event_time_steps(torch, lambda: plan.solve_ir(db, dx, k), args.steps, args.warmup, flush, stream)
-    clocks = sampler.stop() if sampler else None
+    sampler.start()
+    ts = event_time_steps(torch, solve(mode), args.steps, args.warmup, flush, stream)
+    clocks = sampler.stop()
     torch.cuda.synchronize()
     barrier(dist)
     S.sync_status()
     total_ms = reduce_max(dist, sum(ts))
     value = world * k * args.steps / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+    launches_per_step = 1 if mode == 64 else 1 + 2 * ir_iters
 
-    # dominant kernel: the FP32 sync-free solve launch
-    t32 = statistics.median(event_time_steps(torch, lambda: plan.solve_f32(db, dx32, k), max(5, args.steps // 2),
-                                             2, flush, stream))
-    peak, peak_kind = measured_peak()
-    b32 = f32_launch_bytes(n, nnz, k)
-    achieved = b32 / (t32 / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": load_traffic(f"sptrsv_f32_{args.config}"), "kernel": "k_sptrsv<PermMat<float>> (FP32 solve)",
-                "algorithmic_bytes_per_launch": b32, "launch_ms": t32, "peak_kind": peak_kind}
-
-    # plain FP64 sync-free solve (the drop-in path)
+    # --- the other mode and the drop-in FP64 path
+    other = 32 if mode == 64 else 64
+    set_mode(other)
+    t_other = statistics.median(event_time_steps(torch, solve(other), max(5, args.steps // 2), 2, flush, stream))
+    set_mode(mode)
     if k == 1:
-        t64p = event_time_steps(torch, lambda: S.csr_L_solve_multirow(L, info, db, dx, n, stream),
-                                max(5, args.steps // 2), 2, flush, stream)
+        fn_plain = lambda: S.csr_L_solve_multirow(L, info, db, dx, n, stream)  # noqa: E731
     else:
-        t64p = event_time_steps(torch, lambda: plan.solve_f64(db, dx, k), max(5, args.steps // 2), 2, flush, stream)
+        fn_plain = lambda: plan.solve_f64(db, dx, k)  # noqa: E731
+    t_plain = statistics.median(event_time_steps(torch, fn_plain, max(5, args.steps // 2), 2, flush, stream))
     S.sync_status()
-    plain_ms = statistics.median(t64p)
-    plain = {"solves_s": k / (plain_ms / 1e3), "ms": plain_ms,
-             "gb_s": algorithmic_bytes(n, nnz, k) / (plain_ms / 1e3) / 1e9,
-             "path": "csr_L_solve_multirow" if k == 1 else "sptrsv_solve_f64"}
+    err_plain = O.rel_err(dx.cpu().numpy(), ref)
+    set_mode(mode)
 
-    # end to end through the C ABI host-buffer entry point
+    # --- dominant kernel and its roofline
+    peak, peak_kind = measured_peak()
+    if mode == 64:
+        t_kern, bytes_kern = ms_per_step, algorithmic_bytes(n, nnz, k)
+        kname = "sync-free FP64 solve, one launch per solve (sptrsv_solve_f64)"
+    else:
+        t_kern = statistics.median(event_time_steps(torch, lambda: plan.solve_f32(db, dx32, k),
+                                                    max(5, args.steps // 2), 2, flush, stream))
+        bytes_kern = f32_launch_bytes(n, nnz, k)
+        kname = "sync-free FP32 solve (sptrsv_solve_f32), 1 + ir_iters launches per solve"
+    achieved = bytes_kern / (t_kern / 1e3) / 1e9
+    sched = SEL.schedule_from_class(sel64 if mode == 64 else sel32)
+    variant = SEL.VARIANT_NAMES[sched.variant]
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": load_traffic(f"{variant}_{'f64' if mode == 64 else 'f32'}_{args.config}"),
+                "kernel": kname, "algorithmic_bytes_per_launch": bytes_kern, "launch_ms": t_kern,
+                "peak_kind": peak_kind}
+    hops = chain_hop_us(torch, S, SEL)
+    roofline.update(hops)
+    roofline["latency_floor_ms"] = {"nlevs_x_smem_hop": info.nlevs * hops["smem_hop_us"] / 1e3,
+                                    "nlevs_x_l2_hop": info.nlevs * hops["l2_hop_us"] / 1e3}
+
+    # --- end to end through the C ABI host-buffer entry point
     hb = torch.from_numpy(b).pin_memory()
     hx = torch.empty(n * k, dtype=torch.float64).pin_memory()
-    te = event_time_steps(torch, lambda: plan.solve_host(hb, hx, k, 32, stream), max(5, args.steps // 2),
-                          2, flush, stream)
+    te = event_time_steps(torch, lambda: plan.solve_host(hb, hx, k, mode, stream), max(5, args.steps // 2), 2,
+                          flush, stream)
     e2e_ms = reduce_max(dist, sum(te)) / len(te)
     err_e2e = O.rel_err(hx.numpy(), ref)
 
-    ms_per_step = total_ms / args.steps
     gbs = algorithmic_bytes(n, nnz, k) / (ms_per_step / 1e3) / 1e9
     cpu = cpu_baseline_sample(m, b, k) if (rank == 0 and world == 1 and not args.no_cpu) else None
-    sched_names = {0: "simple", 1: "order", 2: "multirow", 3: "cluster"}
+    refk = reference_kernels(args.config) if (rank == 0 and world == 1 and not args.no_ref and k == 1) else None
+    t32 = mode_ms[32] if mode == 64 else ms_per_step
     line = {
         "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64-refine", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if mode == 64 else "f32+f64-refine", "data": "synthetic",
         "config": {"workload": CONFIG_NAMES[args.config], "n": n, "nnz": nnz, "nlevs": info.nlevs, "nrhs": k,
                    "l2": "flushed before every step (256 MiB write)",
-                   "schedule": {"variant": sched_names[best[1]], "rows_per_warp": best[2], "ir_iters": 2},
+                   "schedule": dict(SEL.schedule_from_class(sel64 if mode == 64 else sel32).as_dict(),
+                                    ir_max_iters=ir_iters, name=SEL.class_name(sel64 if mode == 64 else sel32)),
+                   "selected_by": "learned selector (MLP)" if learned else "exhaustive autotuner",
                    "parallelism": f"replicas x{world}"},
-        "gb_s": gbs, "hbm_frac": gbs / peak, "rel_err": {"fp32_ir": err_ir, "fp64": err_f64, "e2e": err_e2e},
-        "plain_fp64": plain, "speedup_vs_plain_fp64": plain_ms / ms_per_step,
+        "gb_s": gbs, "hbm_frac": gbs / peak,
+        "rel_err": {"tuned": errs[mode], "fp64": errs[64], "fp32_refine": errs[32], "plain_fp64": err_plain,
+                    "e2e": err_e2e, "tol": TOL},
+        "fp32_refine": {"solves_s": k / ((t_other if mode == 64 else ms_per_step) / 1e3),
+                        "ms": t_other if mode == 64 else ms_per_step, "ir_iters": ir_iters,
+                        "calibration_ratio": ir_est},
+        "fp64_tuned": {"solves_s": k / ((ms_per_step if mode == 64 else t_other) / 1e3),
+                       "ms": ms_per_step if mode == 64 else t_other},
+        "plain_fp64": {"solves_s": k / (t_plain / 1e3), "ms": t_plain,
+                       "gb_s": algorithmic_bytes(n, nnz, k) / (t_plain / 1e3) / 1e9,
+                       "path": "csr_L_solve_multirow" if k == 1 else "sptrsv_solve_f64 (multirow)"},
+        "speedup_vs_plain_fp64": t_plain / ms_per_step,
+        "fp32_refine_speedup_vs_plain_fp64": t_plain / t32,
+        "autotune": {"best_fp64": {"class": cls64, "name": SEL.class_name(cls64), "ms": float(times64[cls64])},
+                     "best_fp32_refine": {"class": cls32, "name": SEL.class_name(cls32), "ms": float(times32[cls32])},
+                     "seconds": tune_s},
+        "learned_selection": learned,
         "analysis_ms": analysis_ms,
         "e2e": {"value": world * k / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
                 "d2h_bytes_per_step": 8 * n * k},
-        "roofline": roofline, "gpu_launches": (1 + 2 * 2) * args.steps,
-        "clocks": clocks, "cpu_baseline": cpu,
+        "roofline": roofline, "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks, "cpu_baseline": cpu, "reference_kernels": refk,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -368,6 +486,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIG_NAMES), default="c1")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-ref", action="store_true", help="skip the reference-kernel comparators")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -235,6 +235,16 @@ int sptrsv_solve_f64(sptrsv_plan_t plan, const double* b, double* x, int nrhs, c
  * Same layout as sptrsv_solve_f64. */
 int sptrsv_solve_ir(sptrsv_plan_t plan, const double* b, double* x, int nrhs, cudaStream_t stream);
 
+/* Picks the number of refinement steps for this plan: runs the FP32 solve
+ * and corrections (up to max_iters + 1) on b, and sets ir_max_iters to the
+ * fewest steps after which the next correction, relative to x in the
+ * inf-norm, is below tol (the next correction estimates the remaining
+ * forward error; pass a margin, e.g. tol = 1e-13 for a 1e-12 target).
+ * x is a DEVICE scratch/output vector.  *iters and *est (that ratio) may be
+ * NULL.  SPTRSV_ERR_NOT_CONVERGED if max_iters steps do not get there. */
+int sptrsv_plan_calibrate_ir(sptrsv_plan_t plan, const double* b, double* x, int nrhs, double tol, int max_iters,
+                             int* iters, double* est);
+
 /* The inner FP32 solve of sptrsv_solve_ir on its own: x32 (DEVICE, n x nrhs
  * floats) = L^-1 b with FP32 values and accumulation, b read as FP64. */
 int sptrsv_solve_f32(sptrsv_plan_t plan, const double* b, float* x32, int nrhs, cudaStream_t stream);

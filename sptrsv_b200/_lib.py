@@ -100,6 +100,8 @@ _SIGS = {
     "sptrsv_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_ir": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "sptrsv_plan_calibrate_ir": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, c_int, POINTER(c_int),
+                                         POINTER(c_double)]),
     "sptrsv_solve_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "sptrsv_residual_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_ir_noalloc": (c_int, [POINTER(SpMat), c_void_p, c_void_p, c_int, c_void_p]),

@@ -335,6 +335,85 @@ int plan_solve_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaSt
     return 0;
 }
 
+namespace {
+
+// max |a| into *out as the bit pattern of a non-negative float/double (IEEE
+// order of non-negative values is integer order; a NaN reads as the largest)
+__global__ void k_absmax32(const float* __restrict__ a, long long m, unsigned* out)
+{
+    unsigned mx = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        mx = max(mx, __float_as_uint(fabsf(a[i])));
+    for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+__global__ void k_absmax64(const double* __restrict__ a, long long m, unsigned long long* out)
+{
+    unsigned long long mx = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        mx = max(mx, (unsigned long long)__double_as_longlong(fabs(a[i])));
+    for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+}  // namespace
+
+// Runs the refinement with up to max_iters steps and returns in *iters the
+// fewest steps after which the next correction is below tol relative to x
+// (the next correction estimates the remaining error).
+int plan_calibrate_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, double tol, int max_iters,
+                      int* iters, double* last_ratio)
+{
+    int e = plan_ensure_work(p, nrhs);
+    if (e) return e;
+    const long long m = (long long)p->n * nrhs;
+    const size_t bytes32 = sizeof(float) * (size_t)m;
+    unsigned long long* d_n = nullptr;  // [0] |x| (f64 bits), [1] |d| (f32 bits)
+    SPT_CUDA(cudaMalloc((void**)&d_n, 2 * sizeof(unsigned long long)));
+    cudaStream_t s = 0;
+    auto fail = [&](int code) {
+        cudaFree(d_n);
+        return code;
+    };
+    if (cudaMemsetAsync(p->w32a, 0xFF, bytes32, s) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "calibrate"));
+    e = plan_launch<float, float, double, OUT_SET64>(p, true, b, p->w32a, x, nrhs, s);
+    if (e) return fail(e);
+    int need = max_iters;
+    double ratio = 0;
+    for (int it = 1; it <= max_iters + 1; it++) {
+        e = plan_residual(p, b, x, p->w32b, nullptr, nrhs, s);
+        if (e) return fail(e);
+        cudaMemsetAsync(p->w32a, 0xFF, bytes32, s);
+        e = plan_launch<float, float, float, OUT_X>(p, true, p->w32b, p->w32a, nullptr, nrhs, s);
+        if (e) return fail(e);
+        cudaMemsetAsync(d_n, 0, 2 * sizeof(unsigned long long), s);
+        k_absmax64<<<grid_for(m, 256), 256, 0, s>>>(x, m, d_n);
+        k_absmax32<<<grid_for(m, 256), 256, 0, s>>>(p->w32a, m, reinterpret_cast<unsigned*>(d_n + 1));
+        unsigned long long h[2] = {0, 0};
+        if (cudaMemcpyAsync(h, d_n, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return fail(cuda_fail(cudaGetLastError(), "calibrate norms"));
+        e = sync_status(s);
+        if (e) return fail(e);
+        double xn = __builtin_bit_cast(double, h[0]);
+        double dn = (double)__builtin_bit_cast(float, (unsigned)h[1]);
+        ratio = xn > 0 ? dn / xn : dn;
+        if (ratio <= tol) {  // x after it-1 steps is within tol
+            need = it - 1;
+            break;
+        }
+        if (it == max_iters + 1) break;
+        // apply the correction: x += d (the plain solve above wrote d to w32a only)
+        cudaMemsetAsync(p->w32a, 0xFF, bytes32, s);
+        e = plan_launch<float, float, float, OUT_ADD64>(p, true, p->w32b, p->w32a, x, nrhs, s);
+        if (e) return fail(e);
+    }
+    cudaFree(d_n);
+    if (iters) *iters = need;
+    if (last_ratio) *last_ratio = ratio;
+    return 0;
+}
+
 int check_schedule(const sptrsv_schedule_t* s)
 {
     if (s->variant < 0 || s->variant >= SPTRSV_N_VARIANTS)
@@ -505,6 +584,31 @@ int sptrsv_solve_f32(sptrsv_plan_t p, const double* b, float* x32, int nrhs, cud
     SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)p->n * nrhs, stream));
     int e = plan_launch<float, float, double, OUT_X>(p, true, b, x32, nullptr, nrhs, stream);
     return e ? e : ok();
+}
+
+int sptrsv_plan_calibrate_ir(sptrsv_plan_t p, const double* b, double* x, int nrhs, double tol, int max_iters,
+                             int* iters, double* est)
+{
+    if (!p || !b || !x || nrhs < 1 || nrhs > 32 || !(tol > 0) || max_iters < 0 || max_iters > 16)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "calibrate_ir: bad arguments");
+    if (p->n == 0) {
+        if (iters) *iters = 0;
+        return ok();
+    }
+    int need = max_iters;
+    double r = 0;
+    int e = plan_calibrate_ir(p, b, x, nrhs, tol, max_iters, &need, &r);
+    if (e) return e;
+    if (r > tol && need >= max_iters) {
+        p->sched.ir_max_iters = max_iters;
+        if (iters) *iters = need;
+        if (est) *est = r;
+        return set_error(SPTRSV_ERR_NOT_CONVERGED, "calibrate_ir: correction/x = %.3g after %d steps", r, max_iters);
+    }
+    p->sched.ir_max_iters = need;
+    if (iters) *iters = need;
+    if (est) *est = r;
+    return ok();
 }
 
 int sptrsv_residual_f64(sptrsv_plan_t p, const double* b, const double* x, double* r, int nrhs, cudaStream_t stream)

@@ -207,6 +207,14 @@ class Plan:
         m = self.n * nrhs
         C.check(C.lib().sptrsv_solve_ir(self._h, _dev(b, "float64", m), _dev(x, "float64", m), nrhs, _stream(stream)))
 
+    def calibrate_ir(self, b, x, nrhs: int = 1, tol: float = 1e-13, max_iters: int = 4):
+        """Sets and returns the refinement step count for this plan."""
+        m = self.n * nrhs
+        it, est = c_int(0), ctypes.c_double(0)
+        C.check(C.lib().sptrsv_plan_calibrate_ir(self._h, _dev(b, "float64", m), _dev(x, "float64", m), nrhs, tol,
+                                                 max_iters, byref(it), byref(est)))
+        return it.value, est.value
+
     def solve_f32(self, b, x32, nrhs: int = 1, stream=None):
         m = self.n * nrhs
         C.check(C.lib().sptrsv_solve_f32(self._h, _dev(b, "float64", m), _dev(x32, "float32", m), nrhs,

@@ -163,6 +163,28 @@ def test_plan_multi_rhs(torch_cuda, k):
     S.free_device_analysis(L, info)
 
 
+@pytest.mark.parametrize("cfg,k", [("grid", 1), ("zipf", 16)])
+def test_calibrated_refinement_meets_tolerance(torch_cuda, cfg, k):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.grid2d(400, 400, seed=1) if cfg == "grid" else gen.zipf(100000, 1.5, 256, seed=2)
+    xt = gen.vector(m.n * k, "normal", seed=11)
+    b = m.matvec(xt, k)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty_like(db)
+    iters, est = plan.calibrate_ir(db, dx, k, tol=1e-13, max_iters=4)
+    assert 1 <= iters <= 3 and est <= 1e-13
+    assert plan.schedule().ir_max_iters == iters
+    plan.solve_ir(db, dx, k)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k)) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
 def test_value_update_reuses_analysis(torch_cuda):
     import sptrsv_b200 as S
 
