@@ -240,17 +240,22 @@ def reference_kernels(cfg: str, timeout_s: int = 240):
     benchmark down; returns {solver: {"ms": median, "err": rel err}} or None."""
     from oracle import oracle as O
 
-    if not O.ref_available():
-        return None
     code = (
         "import sys, json; sys.path.insert(0, %r)\n"
         "from oracle import oracle as O\nfrom sptrsv_b200 import gen\n"
-        "m, xt, k = gen.config(%r)\nb = m.matvec(xt, k)\nref = O.solve(m.rowptr, m.colidx, m.val, b)\n"
-        "O.ref_lib().ref_set_watchdog_seconds(60.0)\nout = {}\n"
-        "for v, name in ((2, 'multirow'), (1, 'order'), (0, 'simple')):\n"
-        "    x, ms = O.ref_solve(v, m.rowptr, m.colidx, m.val, b, reps=5)\n"
-        "    out[name] = {'ms': ms, 'rel_err': O.rel_err(x, ref)}\n"
-        "    print(json.dumps(out), flush=True)\n" % (str(ROOT), cfg))
+        "m, xt, k = gen.config(%r)\nb = m.matvec(xt, k)\nref = O.solve(m.rowptr, m.colidx, m.val, b)\nout = {}\n"
+        "try:\n"
+        "    x, ms, am = O.cusparse_solve(m.rowptr, m.colidx, m.val, b, reps=5)\n"
+        "    out['cusparse_spsv'] = {'ms': ms, 'analysis_ms': am, 'rel_err': O.rel_err(x, ref)}\n"
+        "except Exception as e:\n"
+        "    out['cusparse_spsv'] = {'note': str(e)[:200]}\n"
+        "print(json.dumps(out), flush=True)\n"
+        "if O.ref_available():\n"
+        "    O.ref_lib().ref_set_watchdog_seconds(60.0)\n"
+        "    for v, name in ((2, 'ref_multirow'), (1, 'ref_order'), (0, 'ref_simple')):\n"
+        "        x, ms = O.ref_solve(v, m.rowptr, m.colidx, m.val, b, reps=5)\n"
+        "        out[name] = {'ms': ms, 'rel_err': O.rel_err(x, ref)}\n"
+        "        print(json.dumps(out), flush=True)\n" % (str(ROOT), cfg))
     try:
         r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout_s)
     except subprocess.TimeoutExpired as e:
@@ -335,13 +340,30 @@ def run_ours(args, rank, world, local, dist):
     def flush():
         flush_buf.fill_(1)
 
+    if args.lean:
+        # profiling run: one fixed schedule, warm-up and the timed steps, nothing else
+        cls = args.fixed_class if args.fixed_class >= 0 else 23
+        s = SEL.schedule_from_class(cls)
+        s.ir_max_iters = 1
+        plan.set_schedule_struct(s)
+        fn = (lambda: plan.solve_f64(db, dx, k)) if args.lean == 64 else (lambda: plan.solve_ir(db, dx, k))
+        ts = event_time_steps(torch, fn, args.steps, args.warmup, flush, stream)
+        S.sync_status()
+        print(json.dumps({"lean": True, "class": SEL.class_name(cls), "precision": args.lean,
+                          "ms_per_step": sum(ts) / len(ts)}), flush=True)
+        plan.close()
+        S.free_device_analysis(L, info)
+        return
+
     # --- schedule: learned selector when trained, exhaustive autotuner beside it
     t0 = time.perf_counter()
     cls64, times64 = SEL.autotune(plan, db, dx, k, 64, reps=3)
     cls32, times32 = SEL.autotune(plan, db, dx, k, 32, reps=3)
     tune_s = time.perf_counter() - t0
     learned = None
-    if SELECTOR_WEIGHTS.exists():
+    if args.fixed_class >= 0:
+        cls64 = cls32 = args.fixed_class
+    elif SELECTOR_WEIGHTS.exists():
         net = SEL.Mlp.load(SELECTOR_WEIGHTS)
         f = SEL.features(L, info)
         c = net.predict_class(f)
@@ -487,6 +509,9 @@ def main():
     ap.add_argument("--config", choices=sorted(CONFIG_NAMES), default="c1")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-ref", action="store_true", help="skip the reference-kernel comparators")
+    ap.add_argument("--fixed-class", type=int, default=-1, help="use this schedule class instead of selecting one")
+    ap.add_argument("--lean", type=int, default=0, choices=[0, 32, 64],
+                    help="profiling run: only the timed solves of --fixed-class at this precision")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

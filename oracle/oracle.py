@@ -209,6 +209,29 @@ def ref_solve(variant: int, rowptr, colidx, val, b, reps: int = 1):
     return x, ms.value
 
 
+CUSPARSE_SO = HERE / "libcusparse_cmp.so"
+
+
+def cusparse_solve(rowptr, colidx, val, b, reps: int = 5):
+    """(x, solve ms, analysis ms) of cusparseSpSV (FP64), the comparator the
+    reference's csrsv2 wrapper (solver/solve_csr_cusparse.cu) maps to."""
+    if not CUSPARSE_SO.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "libcusparse_cmp.so"], check=True)
+    L = ctypes.CDLL(str(CUSPARSE_SO))
+    L.cmp_cusparse_spsv.restype = c_int
+    L.cmp_cusparse_spsv.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                    POINTER(c_float), POINTER(c_float)]
+    rp, ci, va, bb = _i32(rowptr), _i32(colidx), _f64(val), _f64(b)
+    n = rp.shape[0] - 1
+    x = np.zeros(n)
+    sm, am = c_float(0), c_float(0)
+    rc = L.cmp_cusparse_spsv(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, bb.ctypes.data, x.ctypes.data, reps,
+                             ctypes.byref(sm), ctypes.byref(am))
+    if rc != 0:
+        raise RuntimeError(f"cusparse comparator failed ({rc})")
+    return x, sm.value, am.value
+
+
 def timed(fn, *a, **k):
     t0 = time.perf_counter()
     r = fn(*a, **k)

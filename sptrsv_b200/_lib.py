@@ -108,7 +108,7 @@ _SIGS = {
     "sptrsv_batch_create": (c_int, [c_int, POINTER(SpMat), c_void_p, POINTER(c_void_p)]),
     "sptrsv_batch_destroy": (c_int, [c_void_p]),
     "sptrsv_batch_info": (c_int, [c_void_p, c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong)]),
-    "sptrsv_batch_set_schedule": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "sptrsv_batch_set_schedule": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int]),
     "sptrsv_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_batch_solve_graph": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_features": (c_int, [POINTER(SpMat), POINTER(AnalysisInfo), c_void_p]),

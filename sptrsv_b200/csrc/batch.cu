@@ -51,6 +51,25 @@ struct sptrsv_batch_s {
     int ntasks = 0;
     float* w32a = nullptr;
     float* w32b = nullptr;
+    // natural-order chunk schedule: the union CSR without its diagonal
+    int* nptr = nullptr;         // [n+1] off-diagonal offsets per union row
+    int* ncol = nullptr;         // [m] union column
+    double* nval64 = nullptr;
+    float* nval32 = nullptr;
+    double* ndg64 = nullptr;
+    double* ndi64 = nullptr;
+    float* ndi32 = nullptr;
+    int* tsys = nullptr;         // [nchunks] per task: system (tasks in (chunk, system) order)
+    int* tj = nullptr;           // [nchunks] per task: chunk index inside its system
+    int* cdep = nullptr;         // [nchunks] per task: first chunk of the same system it reads
+    int* sys_row0 = nullptr;     // [nsys] first union row
+    int* sys_chunk0 = nullptr;   // [nsys] first flag of the system
+    int* sys_k = nullptr;        // [nsys]
+    long long* sys_off = nullptr;  // [nsys]
+    int* flags = nullptr;        // [nchunks] chunk done flags (1 = done)
+    int* row_sys = nullptr;      // [n] system of each union row
+    int nchunks = 0;
+    int chunked = 1;             // 1: natural-order chunks, 0: level-ordered tasks
     int block_warps = 8, warps_per_sm = 0, backoff_ns = 0, ir_iters = 2;
     // graph cache for one (b, x, precision)
     cudaGraphExec_t gexec = nullptr;
@@ -116,6 +135,107 @@ __global__ void __launch_bounds__(512) k_sptrsv_vk(BatchMat bm, const V* __restr
             if (OUT == 1) x64[xr + k] = (double)r;
             if (OUT == 2) x64[xr + k] += (double)r;
         }
+    }
+}
+
+// Natural-order chunk schedule.  Task t is chunk j of system s: its rows
+// [row0_s + 32j, +32), solved one after another by one warp, lane q owning
+// right-hand side q.  Before its first row the warp waits (warp-convergent,
+// acquire) for the done flags of the chunks of the same system that the
+// chunk reads (cdep[t] .. j-1); after that every outside value is final.
+// Values of earlier rows of the chunk come from the warp's shared-memory
+// ring.  When the chunk is done the warp releases its flag.
+struct NatBatch {
+    const int* __restrict__ ptr;
+    const int* __restrict__ col;
+    const int* __restrict__ tsys;
+    const int* __restrict__ tj;
+    const int* __restrict__ cdep;
+    const int* __restrict__ row0;
+    const int* __restrict__ chunk0;
+    const int* __restrict__ sk;
+    const long long* __restrict__ soff;
+};
+
+template <typename V, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(256) k_sptrsv_vkc(NatBatch nb, const V* __restrict__ val, const V* __restrict__ di,
+                                                    int ntasks, int* flags, const BT* __restrict__ b, T* x,
+                                                    double* x64, DevStatus* st, unsigned long long budget,
+                                                    unsigned backoff)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    T* ring = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * 32 * 32;  // [row][rhs]
+    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    for (int t = gw; t < ntasks; t += nw) {
+        const int s = __ldg(nb.tsys + t), j = __ldg(nb.tj + t);
+        const int row0 = __ldg(nb.row0 + s), c0 = __ldg(nb.chunk0 + s), K = __ldg(nb.sk + s);
+        const long long off = __ldg(nb.soff + s);
+        const int nrows_s = __ldg(nb.row0 + s + 1) - row0;
+        const int r0 = row0 + 32 * j, cnt = min(32, row0 + nrows_s - r0);
+        // wait for the chunks this one reads
+        for (int q = __ldg(nb.cdep + t) + lane; __any_sync(0xffffffffu, q < j); q += 32) {
+            int fv = 1;
+            if (!warp_wait<false, int>(q < j, c0 + q, flags, nullptr, fv, st, budget, backoff, r0)) return;
+        }
+        __threadfence();  // acquire: the flagged chunks' x values are visible
+        const bool lk = lane < K;
+        for (int i = 0; i < cnt; i++) {
+            const int r = r0 + i;
+            const long long xr = off + (long long)(r - row0) * K;
+            T acc = lk ? (T)b[xr + lane] : (T)0;
+            const T piv = (T)__ldg(di + r);
+            const int e0 = __ldg(nb.ptr + r), e1 = __ldg(nb.ptr + r + 1);
+            for (int p0 = e0; p0 < e1; p0 += 32) {
+                const int nq = min(32, e1 - p0);
+                int c = 0;
+                T v = 0;
+                if (lane < nq) {
+                    c = __ldg(nb.col + p0 + lane);
+                    v = (T)__ldg(val + p0 + lane);
+                }
+#pragma unroll 4
+                for (int u = 0; u < nq; u++) {
+                    const int cu = __shfl_sync(0xffffffffu, c, u);
+                    const T vu = __shfl_sync(0xffffffffu, v, u);
+                    T xv = 0;
+                    if (lk) xv = cu >= r0 ? ring[(cu - r0) * 32 + lane] : ld_relaxed(x + off + (long long)(cu - row0) * K + lane);
+                    acc -= vu * xv;
+                }
+            }
+            if (lk) {
+                const T res = publishable(acc * piv);
+                ring[i * 32 + lane] = res;
+                st_relaxed(x + xr + lane, res);
+                if (OUT == 1) x64[xr + lane] = (double)res;
+                if (OUT == 2) x64[xr + lane] += (double)res;
+            }
+            __syncwarp();
+        }
+        __threadfence();  // release: this chunk's x values before its flag
+        if (lane == 0) st_relaxed(flags + c0 + j, 1);
+    }
+}
+
+// r = b - L x in FP64 over the natural-order union, one warp per row, lanes over the right-hand sides
+__global__ void __launch_bounds__(256) k_residual_vkc(const int* __restrict__ ptr, const int* __restrict__ col,
+                                                      const double* __restrict__ val, const double* __restrict__ dg,
+                                                      const int* __restrict__ row_sys, const int* __restrict__ row0,
+                                                      const int* __restrict__ sk, const long long* __restrict__ soff,
+                                                      int n, const double* __restrict__ b,
+                                                      const double* __restrict__ x, float* __restrict__ r)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const int s = row_sys[i], K = sk[s], r0 = row0[s];
+        if (lane >= K) continue;
+        const long long o = soff[s];
+        const long long xr = o + (long long)(i - r0) * K + lane;
+        double acc = b[xr] - dg[i] * x[xr];
+        for (int p = ptr[i]; p < ptr[i + 1]; p++) acc -= val[p] * x[o + (long long)(col[p] - r0) * K + lane];
+        r[xr] = (float)acc;
     }
 }
 
@@ -210,6 +330,53 @@ __global__ void k_batch_fill(const int* __restrict__ order, const int* __restric
     }
 }
 
+// natural-order union without diagonals: nptr[i] = ia[i] - i (one diagonal per earlier row)
+__global__ void k_nat_fill(const int* __restrict__ urp, const int* __restrict__ uci, const double* __restrict__ uva,
+                           int n, int* __restrict__ nptr, int* __restrict__ ncol, double* __restrict__ nval64,
+                           float* __restrict__ nval32, double* __restrict__ ndg, double* __restrict__ ndi,
+                           float* __restrict__ ndi32)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const int a = urp[i], e = urp[i + 1] - 1, o = a - (int)i;
+        for (int q = a + lane; q < e; q += 32) {
+            ncol[o + q - a] = uci[q];
+            nval64[o + q - a] = uva[q];
+            nval32[o + q - a] = (float)uva[q];
+        }
+        if (lane == 0) {
+            const double d = uva[e];
+            nptr[i] = o;
+            ndg[i] = d;
+            ndi[i] = 1.0 / d;
+            ndi32[i] = 1.0f / (float)d;
+            if (i == n - 1) nptr[n] = e - (int)i;
+        }
+    }
+}
+
+// first chunk each natural chunk reads: the chunk of its smallest column
+__global__ void k_chunk_dep(const int* __restrict__ nptr, const int* __restrict__ ncol,
+                            const int* __restrict__ chunk0, const int* __restrict__ row0, int nsys, int nchunks,
+                            int* __restrict__ dep)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        int lo = 0, hi = nsys - 1;  // system: largest s with chunk0[s] <= c
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (chunk0[mid] <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const int s = lo, j = c - chunk0[s];
+        const int r0 = row0[s] + 32 * j, r1 = min(r0 + 32, row0[s + 1]);
+        int mn = r0;
+        for (int r = r0; r < r1; r++)
+            if (nptr[r + 1] > nptr[r]) mn = min(mn, ncol[nptr[r]]);
+        dep[c] = (mn - row0[s]) / 32;
+    }
+}
+
 __global__ void k_task_kp(const int* __restrict__ tbase, int ntasks, const int* __restrict__ key_sorted,
                           int* __restrict__ tkp)
 {
@@ -221,6 +388,10 @@ void batch_free(sptrsv_batch_s* B)
 {
     if (B->gexec) cudaGraphExecDestroy(B->gexec);
     if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+    cudaFree(B->nptr); cudaFree(B->ncol); cudaFree(B->nval64); cudaFree(B->nval32); cudaFree(B->ndg64);
+    cudaFree(B->ndi64); cudaFree(B->ndi32); cudaFree(B->tsys); cudaFree(B->tj); cudaFree(B->cdep);
+    cudaFree(B->sys_row0); cudaFree(B->sys_chunk0); cudaFree(B->sys_k); cudaFree(B->sys_off); cudaFree(B->flags);
+    cudaFree(B->row_sys);
     cudaFree(B->ptr); cudaFree(B->xrow); cudaFree(B->krow); cudaFree(B->xdep); cudaFree(B->val64);
     cudaFree(B->val32); cudaFree(B->dg64); cudaFree(B->di64); cudaFree(B->di32); cudaFree(B->tbase);
     cudaFree(B->tkp); cudaFree(B->w32a); cudaFree(B->w32b);
@@ -241,16 +412,47 @@ int batch_tasks(sptrsv_batch_s* B, const int* key_sorted, int K, cudaStream_t s)
 }
 
 template <typename V, typename T, typename BT, int OUT>
-int batch_launch(sptrsv_batch_s* B, const V* val, const V* di, const BT* b, T* x, double* x64, cudaStream_t s)
+int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cudaStream_t s)
 {
     Ctx* c = ctx();
-    BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
     const int block = 32 * B->block_warps;
     const int cap = B->warps_per_sm > 0 ? (B->warps_per_sm + B->block_warps - 1) / B->block_warps : 0;
+    if (B->chunked) {
+        const V* val = f32 ? reinterpret_cast<const V*>(B->nval32) : reinterpret_cast<const V*>(B->nval64);
+        const V* di = f32 ? reinterpret_cast<const V*>(B->ndi32) : reinterpret_cast<const V*>(B->ndi64);
+        NatBatch nb{B->nptr, B->ncol, B->tsys, B->tj, B->cdep, B->sys_row0, B->sys_chunk0, B->sys_k, B->sys_off};
+        SPT_CUDA(cudaMemsetAsync(B->flags, 0, sizeof(int) * (size_t)B->nchunks, s));
+        auto kern = k_sptrsv_vkc<V, T, BT, OUT>;
+        const size_t smem = (size_t)B->block_warps * 32 * 32 * sizeof(T);
+        if (smem > 48 * 1024)
+            SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(B->nchunks, B->block_warps), cap, s, nb, val, di,
+                                          B->nchunks, B->flags, b, x, x64, c->d_status, wait_budget_ns(),
+                                          (unsigned)B->backoff_ns));
+        return 0;
+    }
+    const V* val = f32 ? reinterpret_cast<const V*>(B->val32) : reinterpret_cast<const V*>(B->val64);
+    const V* di = f32 ? reinterpret_cast<const V*>(B->di32) : reinterpret_cast<const V*>(B->di64);
+    BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
     auto kern = k_sptrsv_vk<V, T, BT, OUT>;
     SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(B->ntasks, B->block_warps), cap, s, bm, val, di,
                                       B->ntasks, (const int*)B->tbase, (const int*)B->tkp, b, x, x64, c->d_status,
                                       wait_budget_ns(), (unsigned)B->backoff_ns));
+    return 0;
+}
+
+int batch_residual(sptrsv_batch_s* B, const double* b, const double* x, cudaStream_t s)
+{
+    if (B->chunked) {
+        k_residual_vkc<<<grid_for((long long)B->n * 32, 256), 256, 0, s>>>(B->nptr, B->ncol, B->nval64, B->ndg64,
+                                                                          B->row_sys, B->sys_row0, B->sys_k,
+                                                                          B->sys_off, B->n, b, x, B->w32b);
+    } else {
+        BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
+        k_residual_vk<<<grid_for((long long)B->ntasks * 32, 256), 256, 0, s>>>(bm, B->val64, B->dg64, B->ntasks,
+                                                                                B->tbase, B->tkp, b, x, B->w32b);
+    }
+    SPT_CUDA(cudaGetLastError());
     return 0;
 }
 
@@ -259,19 +461,17 @@ int batch_solve_impl(sptrsv_batch_s* B, const double* b, double* x, int precisio
     if (B->n == 0) return 0;
     if (precision == 64) {
         SPT_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(double) * (size_t)B->nvec, s));
-        return batch_launch<double, double, double, 0>(B, B->val64, B->di64, b, x, nullptr, s);
+        return batch_launch<double, double, double, 0>(B, false, b, x, nullptr, s);
     }
     const size_t b32 = sizeof(float) * (size_t)B->nvec;
     SPT_CUDA(cudaMemsetAsync(B->w32a, 0xFF, b32, s));
-    int e = batch_launch<float, float, double, 1>(B, B->val32, B->di32, b, B->w32a, x, s);
+    int e = batch_launch<float, float, double, 1>(B, true, b, B->w32a, x, s);
     if (e) return e;
-    BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
     for (int it = 0; it < B->ir_iters; it++) {
-        k_residual_vk<<<grid_for((long long)B->ntasks * 32, 256), 256, 0, s>>>(bm, B->val64, B->dg64, B->ntasks,
-                                                                                B->tbase, B->tkp, b, x, B->w32b);
-        SPT_CUDA(cudaGetLastError());
+        e = batch_residual(B, b, x, s);
+        if (e) return e;
         SPT_CUDA(cudaMemsetAsync(B->w32a, 0xFF, b32, s));
-        e = batch_launch<float, float, float, 2>(B, B->val32, B->di32, B->w32b, B->w32a, x, s);
+        e = batch_launch<float, float, float, 2>(B, true, B->w32b, B->w32a, x, s);
         if (e) return e;
     }
     return 0;
@@ -411,6 +611,65 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
         int e = batch_tasks(B, key, 6 * info.nlevs, s);
         if (e) return fail(e);
     }
+    // 5. natural-order chunk schedule: union without diagonals, chunk tasks in
+    //    (chunk index, system) order, each with the first chunk it reads
+    BCHK(dalloc(&B->nptr, n + 1));
+    BCHK(dalloc(&B->ncol, B->m));
+    BCHK(dalloc(&B->nval64, B->m));
+    BCHK(dalloc(&B->nval32, B->m));
+    BCHK(dalloc(&B->ndg64, n));
+    BCHK(dalloc(&B->ndi64, n));
+    BCHK(dalloc(&B->ndi32, n));
+    k_nat_fill<<<grid_for(n * 32, 256), 256, 0, s>>>(U.ia, U.ja, U.a, (int)n, B->nptr, B->ncol, B->nval64, B->nval32,
+                                                      B->ndg64, B->ndi64, B->ndi32);
+    BCHK(cudaGetLastError());
+    {
+        std::vector<int> chunk0(nsys + 1), nch(nsys);
+        int maxch = 0;
+        chunk0[0] = 0;
+        for (int k = 0; k < nsys; k++) {
+            nch[k] = (mats[k].nr + 31) / 32;
+            chunk0[k + 1] = chunk0[k] + nch[k];
+            maxch = std::max(maxch, nch[k]);
+        }
+        B->nchunks = chunk0[nsys];
+        BCHK(dalloc(&B->sys_row0, nsys + 1));
+        BCHK(dalloc(&B->sys_chunk0, nsys + 1));
+        BCHK(dalloc(&B->sys_k, nsys));
+        BCHK(dalloc(&B->sys_off, nsys + 1));
+        BCHK(cudaMemcpy(B->sys_row0, row0.data(), sizeof(int) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->sys_chunk0, chunk0.data(), sizeof(int) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->sys_k, nrhs, sizeof(int) * (size_t)nsys, cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->sys_off, B->off.data(), sizeof(long long) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
+        int* dep_nat = nullptr;
+        BCHK(dalloc(&dep_nat, B->nchunks));
+        k_chunk_dep<<<grid_for(B->nchunks, 256), 256, 0, s>>>(B->nptr, B->ncol, B->sys_chunk0, B->sys_row0, nsys,
+                                                               B->nchunks, dep_nat);
+        std::vector<int> dn(B->nchunks);
+        cudaError_t ce = cudaMemcpy(dn.data(), dep_nat, sizeof(int) * (size_t)B->nchunks, cudaMemcpyDeviceToHost);
+        cudaFree(dep_nat);
+        BCHK(ce);
+        std::vector<int> ts, tjv, td;
+        ts.reserve(B->nchunks);
+        tjv.reserve(B->nchunks);
+        td.reserve(B->nchunks);
+        for (int j = 0; j < maxch; j++)
+            for (int k = 0; k < nsys; k++)
+                if (j < nch[k]) {
+                    ts.push_back(k);
+                    tjv.push_back(j);
+                    td.push_back(dn[chunk0[k] + j]);
+                }
+        BCHK(dalloc(&B->tsys, B->nchunks));
+        BCHK(dalloc(&B->tj, B->nchunks));
+        BCHK(dalloc(&B->cdep, B->nchunks));
+        BCHK(dalloc(&B->flags, B->nchunks));
+        BCHK(cudaMemcpy(B->tsys, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->tj, tjv.data(), sizeof(int) * tjv.size(), cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->cdep, td.data(), sizeof(int) * td.size(), cudaMemcpyHostToDevice));
+    }
+    B->row_sys = d_sys;  // kept for the natural-order residual
+    d_sys = nullptr;
     BCHK(dalloc(&B->w32a, B->nvec));
     BCHK(dalloc(&B->w32b, B->nvec));
     BCHK(cudaStreamSynchronize(s));
@@ -439,11 +698,15 @@ int sptrsv_batch_info(sptrsv_batch_t B, long long* offsets, int* n_total, int* n
     return ok();
 }
 
-int sptrsv_batch_set_schedule(sptrsv_batch_t B, int block_warps, int warps_per_sm, int backoff_ns, int ir_iters)
+int sptrsv_batch_set_schedule(sptrsv_batch_t B, int chunked, int block_warps, int warps_per_sm, int backoff_ns,
+                              int ir_iters)
 {
-    if (!B || (block_warps != 2 && block_warps != 4 && block_warps != 8 && block_warps != 16) || warps_per_sm < 0 ||
-        warps_per_sm > 64 || backoff_ns < 0 || backoff_ns > 100000 || ir_iters < 0 || ir_iters > 16)
+    if (!B || (chunked != 0 && chunked != 1) ||
+        (block_warps != 2 && block_warps != 4 && block_warps != 8 && block_warps != 16) ||
+        (chunked && block_warps > 8) || warps_per_sm < 0 || warps_per_sm > 64 || backoff_ns < 0 ||
+        backoff_ns > 100000 || ir_iters < 0 || ir_iters > 16)
         return set_error(SPTRSV_ERR_INVALID_ARG, "batch_set_schedule: bad arguments");
+    B->chunked = chunked;
     B->block_warps = block_warps;
     B->warps_per_sm = warps_per_sm;
     B->backoff_ns = backoff_ns;

@@ -31,7 +31,8 @@ def test_batch_matches_oracle_per_system(torch_cuda, precision):
     assert np.array_equal(np.diff(batch.offsets), [m.n * k for m, k in zip(mats, ks)])
     db = torch.from_numpy(np.concatenate(bs)).cuda()
     dx = torch.empty_like(db)
-    for sched in (dict(), dict(block_warps=4, warps_per_sm=16), dict(block_warps=16, backoff_ns=100)):
+    for sched in (dict(), dict(chunked=1, block_warps=4, warps_per_sm=16), dict(chunked=0),
+                  dict(chunked=0, block_warps=4, warps_per_sm=16), dict(chunked=0, block_warps=16, backoff_ns=100)):
         batch.set_schedule(**sched)
         batch.solve(db, dx, precision)
         S.sync_status()
