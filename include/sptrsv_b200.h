@@ -379,6 +379,13 @@ int sptrsv_gen_zipf(int n, double s, int max_off, uint64_t seed, sptrsv_host_csr
 /* Block diagonal with dense lower-triangular blocks; diagonally dominant. */
 int sptrsv_gen_blockdiag(int n, int block, uint64_t seed, sptrsv_host_csr_t* out);
 void sptrsv_host_csr_free(sptrsv_host_csr_t* m);
+/* MatrixMarket coordinate file (real/integer/pattern; general, symmetric or
+ * skew-symmetric) -> the lower triangle as CSR with sorted columns and the
+ * diagonal last in every row (added where the file has none), the extraction
+ * of the reference's driver (main.cu:66-246).  unit_values = 1 sets every
+ * value to 1.0 as the reference does (main.cu:228,236); 0 keeps the file's
+ * values (a missing diagonal gets 1.0).  Duplicates are summed. */
+int sptrsv_read_mtx_lower(const char* path, int unit_values, sptrsv_host_csr_t* out);
 /* dist 0: ones, 1: U(-1,1), 2: N(0,1). */
 int sptrsv_gen_vector(long long m, int dist, uint64_t seed, double* out);
 /* y = L x on the host, row-major nrhs. */

@@ -133,6 +133,7 @@ _SIGS = {
     "sptrsv_gen_zipf": (c_int, [c_int, c_double, c_int, c_uint64, POINTER(HostCsr)]),
     "sptrsv_gen_blockdiag": (c_int, [c_int, c_int, c_uint64, POINTER(HostCsr)]),
     "sptrsv_host_csr_free": (None, [POINTER(HostCsr)]),
+    "sptrsv_read_mtx_lower": (c_int, [c_char_p, c_int, POINTER(HostCsr)]),
     "sptrsv_gen_vector": (c_int, [c_longlong, c_int, c_uint64, c_void_p]),
     "sptrsv_host_spmv": (c_int, [POINTER(HostCsr), c_void_p, c_void_p, c_int]),
 }

@@ -84,6 +84,12 @@ def vector(m: int, dist: str = "ones", seed: int = 0) -> np.ndarray:
     return out
 
 
+def read_mtx_lower(path, unit_values: bool = True) -> HostCsr:
+    """Lower triangle (diagonal last) of a MatrixMarket file; unit_values
+    reproduces the reference driver's all-ones values."""
+    return _take(C.lib().sptrsv_read_mtx_lower, str(path).encode(), 1 if unit_values else 0)
+
+
 def from_arrays(rowptr, colidx, val) -> HostCsr:
     return HostCsr(np.ascontiguousarray(rowptr, np.int32), np.ascontiguousarray(colidx, np.int32),
                    np.ascontiguousarray(val, np.float64))
