@@ -112,12 +112,16 @@ class ClockSampler:
             self.proc.kill()
         rows = [ln.split(",") for ln in Path(self.path).read_text().splitlines() if ln.strip()]
         os.unlink(self.path)
-        sm, smax, reasons = [], 0.0, set()
+        sm, smax, reasons, pw = [], 0.0, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
                 sm.append(float(r[1]))
                 smax = max(smax, float(r[2]))
+                try:
+                    pw.append(float(r[3]))
+                except ValueError:
+                    pass
                 for nm, v in zip(names, r[5:9]):
                     if v.strip().lower() == "active":
                         reasons.add(nm)
@@ -126,7 +130,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_mean": statistics.mean(pw) if pw else None}
 
 
 def dist_setup(args):
@@ -490,6 +494,8 @@ def run_ours(args, rank, world, local, dist):
         "analysis_ms": analysis_ms,
         "e2e": {"value": world * k / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
                 "d2h_bytes_per_step": 8 * n * k},
+        "energy_j_per_solve": (clocks["power_w_mean"] * ms_per_step / 1e3 / k
+                               if clocks and clocks.get("power_w_mean") else None),
         "roofline": roofline, "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks, "cpu_baseline": cpu, "reference_kernels": refk,
     }

@@ -152,26 +152,40 @@ def mlp_gradient(params, mean, std, X, T, M):
 
 
 # ---- the reference's own kernels (GPU only; built by `make -C oracle ref`) ----
-def ref_available() -> bool:
-    return REF_SO.exists()
+REF32_SO = HERE / "_ref" / "libsptrsv_ref_f32.so"
+_r32 = None
 
 
-def ref_lib():
-    global _r
+def ref_available(f32: bool = False) -> bool:
+    return (REF32_SO if f32 else REF_SO).exists()
+
+
+def ref_lib(f32: bool = False):
+    """The reference's kernels; f32 selects its VALUE_TYPE=float build (Makefile:7)."""
+    global _r, _r32
+    if f32:
+        if _r32 is None:
+            if not REF32_SO.exists():
+                raise FileNotFoundError(f"{REF32_SO} not built (make -C oracle ref32)")
+            _r32 = _bind_ref(ctypes.CDLL(str(REF32_SO)))
+        return _r32
     if _r is None:
         if not REF_SO.exists():
             raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref, needs the reference sources)")
-        L = ctypes.CDLL(str(REF_SO))
-        L.ref_analysis.restype = c_int
-        L.ref_analysis.argtypes = [c_int, c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_int), c_void_p,
-                                   c_void_p, c_void_p, c_void_p]
-        L.ref_solve.restype = c_int
-        L.ref_solve.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
-                                POINTER(c_float)]
-        L.ref_set_watchdog_seconds.restype = None
-        L.ref_set_watchdog_seconds.argtypes = [c_double]
-        _r = L
+        _r = _bind_ref(ctypes.CDLL(str(REF_SO)))
     return _r
+
+
+def _bind_ref(L):
+    L.ref_analysis.restype = c_int
+    L.ref_analysis.argtypes = [c_int, c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_int), c_void_p,
+                               c_void_p, c_void_p, c_void_p]
+    L.ref_solve.restype = c_int
+    L.ref_solve.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                            POINTER(c_float)]
+    L.ref_set_watchdog_seconds.restype = None
+    L.ref_set_watchdog_seconds.argtypes = [c_double]
+    return L
 
 
 def ref_analysis(rowptr, colidx, mode: int = 2) -> dict:
@@ -195,9 +209,10 @@ def ref_analysis(rowptr, colidx, mode: int = 2) -> dict:
     return out
 
 
-def ref_solve(variant: int, rowptr, colidx, val, b, reps: int = 1):
-    """(x, median ms) of the reference solver 0 simple, 1 order, 2 multirow."""
-    L = ref_lib()
+def ref_solve(variant: int, rowptr, colidx, val, b, reps: int = 1, f32: bool = False):
+    """(x, median ms) of the reference solver 0 simple, 1 order, 2 multirow
+    (f32: its VALUE_TYPE=float build; values and b rounded to float)."""
+    L = ref_lib(f32)
     rp, ci, va, bb = _i32(rowptr), _i32(colidx), _f64(val), _f64(b)
     n = rp.shape[0] - 1
     x = np.zeros(n, dtype=np.float64)

@@ -116,15 +116,16 @@ static int upload(int n, const int* rowptr, const int* colidx, const double* val
     rp.push_back(rp[n]);
     std::vector<int> ci(colidx, colidx + nnz);
     ci.resize((size_t)nnz + 64, 0);
-    std::vector<double> va((size_t)nnz + 64, 0.0);
-    if (val) std::copy(val, val + nnz, va.begin());
-    else std::fill(va.begin(), va.begin() + nnz, 1.0);
+    // values in the build's VALUE_TYPE (double, or float for the reference's FP32 build)
+    std::vector<VALUE_TYPE> va((size_t)nnz + 64, (VALUE_TYPE)0);
+    if (val) std::transform(val, val + nnz, va.begin(), [](double v) { return (VALUE_TYPE)v; });
+    else std::fill(va.begin(), va.begin() + nnz, (VALUE_TYPE)1);
     if (cudaMalloc((void**)&d->m.ia, sizeof(int) * (n + 2)) != cudaSuccess) return -4;
     if (cudaMalloc((void**)&d->m.ja, sizeof(int) * ci.size()) != cudaSuccess) return -4;
-    if (cudaMalloc((void**)&d->m.a, sizeof(double) * va.size()) != cudaSuccess) return -4;
+    if (cudaMalloc((void**)&d->m.a, sizeof(VALUE_TYPE) * va.size()) != cudaSuccess) return -4;
     cudaMemcpy(d->m.ia, rp.data(), sizeof(int) * (n + 2), cudaMemcpyHostToDevice);
     cudaMemcpy(d->m.ja, ci.data(), sizeof(int) * ci.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(d->m.a, va.data(), sizeof(double) * va.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d->m.a, va.data(), sizeof(VALUE_TYPE) * va.size(), cudaMemcpyHostToDevice);
     d->m.nr = n;
     d->m.nc = n;
     d->m.nnz = nnz;
@@ -217,19 +218,22 @@ extern "C" int ref_solve(int variant, int n, const int* rowptr, const int* colid
         multirow_analysis_base_GPU(&info, &d.m, info_s.mode);
         cudaDeviceSynchronize();
     }
-    double *d_b = nullptr, *d_x = nullptr;
+    VALUE_TYPE *d_b = nullptr, *d_x = nullptr;
     int* is_solved = nullptr;
-    cudaMalloc((void**)&d_b, sizeof(double) * (n + 64));
-    cudaMalloc((void**)&d_x, sizeof(double) * (n + 64));
+    cudaMalloc((void**)&d_b, sizeof(VALUE_TYPE) * (n + 64));
+    cudaMalloc((void**)&d_x, sizeof(VALUE_TYPE) * (n + 64));
     cudaMalloc((void**)&is_solved, sizeof(int) * (n + 64));
-    cudaMemcpy(d_b, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+    {
+        std::vector<VALUE_TYPE> hb(b, b + n);
+        cudaMemcpy(d_b, hb.data(), sizeof(VALUE_TYPE) * n, cudaMemcpyHostToDevice);
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::vector<float> ts;
     if (reps < 1) reps = 1;
     for (int r = 0; r < reps; r++) {
-        cudaMemset(d_x, 0, sizeof(double) * n);
+        cudaMemset(d_x, 0, sizeof(VALUE_TYPE) * n);
         Watchdog wd(variant == 0 ? "csr_L_solve_simple" : variant == 1 ? "csr_L_solve_order" : "csr_L_solve_multirow");
         cudaEventRecord(e0, 0);
         if (variant == 0) csr_L_solve_simple(&d.m, d_b, d_x, n, is_solved);
@@ -242,7 +246,11 @@ extern "C" int ref_solve(int variant, int n, const int* rowptr, const int* colid
         ts.push_back(ms);
     }
     cudaError_t e = cudaGetLastError();
-    cudaMemcpy(x, d_x, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    {
+        std::vector<VALUE_TYPE> hx(n);
+        cudaMemcpy(hx.data(), d_x, sizeof(VALUE_TYPE) * n, cudaMemcpyDeviceToHost);
+        std::copy(hx.begin(), hx.end(), x);
+    }
     std::sort(ts.begin(), ts.end());
     if (ms_median) *ms_median = ts[ts.size() / 2];
     cudaEventDestroy(e0);
