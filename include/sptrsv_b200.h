@@ -290,9 +290,9 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
 int sptrsv_batch_destroy(sptrsv_batch_t batch);
 /* offsets[nsys+1] (may be NULL), total rows, levels of the union, packed length. */
 int sptrsv_batch_info(sptrsv_batch_t batch, long long* offsets, int* n_total, int* nlevs, long long* vec_len);
-/* chunked = 1 (default): each warp takes 32 consecutive rows of one system and
- * solves them in sequence (suits banded and other deep, narrow systems);
- * chunked = 0: level-ordered tasks over the union (suits wide levels).
+/* chunked = 0 (default): level-ordered tasks over the union;
+ * chunked = 1: each warp takes 32 consecutive rows of one system and solves
+ * them in sequence, waiting once per chunk for the chunks it reads.
  * block_warps 2..16 (2..8 when chunked). */
 int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int chunked, int block_warps, int warps_per_sm,
                               int backoff_ns, int ir_iters);

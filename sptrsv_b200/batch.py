@@ -27,7 +27,7 @@ class Batch:
         C.check(C.lib().sptrsv_batch_info(h, off.ctypes.data, byref(n), byref(nl), byref(vl)))
         self.offsets, self.n, self.nlevs, self.vec_len = off, n.value, nl.value, vl.value
 
-    def set_schedule(self, chunked: int = 1, block_warps: int = 8, warps_per_sm: int = 0, backoff_ns: int = 0,
+    def set_schedule(self, chunked: int = 0, block_warps: int = 8, warps_per_sm: int = 0, backoff_ns: int = 0,
                      ir_iters: int = 2):
         C.check(C.lib().sptrsv_batch_set_schedule(self._h, chunked, block_warps, warps_per_sm, backoff_ns, ir_iters))
 

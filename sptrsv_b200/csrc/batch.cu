@@ -69,7 +69,7 @@ struct sptrsv_batch_s {
     int* flags = nullptr;        // [nchunks] chunk done flags (1 = done)
     int* row_sys = nullptr;      // [n] system of each union row
     int nchunks = 0;
-    int chunked = 1;             // 1: natural-order chunks, 0: level-ordered tasks
+    int chunked = 0;             // 0: level-ordered tasks (default), 1: natural-order chunks
     int block_warps = 8, warps_per_sm = 0, backoff_ns = 0, ir_iters = 2;
     // graph cache for one (b, x, precision)
     cudaGraphExec_t gexec = nullptr;
