@@ -52,6 +52,8 @@ CONFIG_NAMES = {
     "c1": "2D 5-point lower triangle 2048x2048, n=4194304, 1 RHS",
     "c2": "Zipf(1.5) DAG n=2000000 (<=256 off-diagonals), 1 RHS",
     "c2k16": "Zipf(1.5) DAG n=2000000 (<=256 off-diagonals), 16 RHS",
+    "c3": "batch of 512 banded systems, n log-uniform [1e3, 2e5], bandwidth log-uniform [16, 4096], "
+          "4-16 off-diagonals per row, 1-32 RHS each, one persistent launch replayed as a CUDA graph",
 }
 TOL = 1e-12
 SELECTOR_WEIGHTS = ROOT / "sptrsv_b200" / "selector_weights.npz"
@@ -177,6 +179,9 @@ def run_reference(args, rank, world, dist):
     from oracle import oracle as O
     from sptrsv_b200 import gen
 
+    if args.config == "c3":
+        run_reference_batch(args, world, dist)
+        return
     m, xt, k = gen.config(args.config)
     b = m.matvec(xt, k)
     a = O.analysis(m.rowptr, m.colidx)
@@ -202,6 +207,53 @@ def run_reference(args, rank, world, dist):
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gb_s": algorithmic_bytes(m.n, m.nnz, k) * v / 1e9, "rel_err_vs_serial": err,
+    }
+    print(json.dumps(line), flush=True)
+    barrier(dist)
+
+
+def run_reference_batch(args, world, dist):
+    """Batched configuration on the host cores: each system's level-scheduled
+    FP64 substitution on all threads, systems one after another; a step is a
+    bounded sample (systems in order until about 2 s), value = RHS solved / s."""
+    from oracle import oracle as O
+    from sptrsv_b200 import gen
+
+    mats, ks, xs = gen.batch_config(512, seed=3)
+    threads = O.num_threads()
+    prep = []
+    for m, x, k in zip(mats, xs, ks):
+        a = O.analysis(m.rowptr, m.colidx)
+        lev_ptr = np.concatenate([[0], np.cumsum(np.bincount(a["levels"] - 1, minlength=a["nlevs"]))]).astype(np.int32)
+        prep.append((m, m.matvec(x, k), k, a, lev_ptr))
+
+    def step():
+        done, t = 0, 0.0
+        for m, b, k, a, lp in prep:
+            t0 = time.perf_counter()
+            O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lp, a["nlevs"], k)
+            t += time.perf_counter() - t0
+            done += k
+            if t > 2.0:
+                break
+        return done, t
+
+    for _ in range(args.warmup):
+        step()
+    done, total = 0, 0.0
+    for _ in range(args.steps):
+        d, t = step()
+        done += d
+        total += t
+    v = done / total
+    sample = f"{args.steps} steps, each the first systems of the batch in order until 2 s (level-scheduled)"
+    line = {
+        "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": CONFIG_NAMES["c3"], "systems": len(mats), "rhs_total": int(sum(ks))},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     barrier(dist)
@@ -346,7 +398,7 @@ def run_ours(args, rank, world, local, dist):
 
     if args.lean:
         # profiling run: one fixed schedule, warm-up and the timed steps, nothing else
-        cls = args.fixed_class if args.fixed_class >= 0 else 23
+        cls = args.fixed_class if args.fixed_class >= 0 else 21  # cluster/H256-B4096-rpw16-bw16
         s = SEL.schedule_from_class(cls)
         s.ir_max_iters = 1
         plan.set_schedule_struct(s)
@@ -369,8 +421,7 @@ def run_ours(args, rank, world, local, dist):
         cls64 = cls32 = args.fixed_class
     elif SELECTOR_WEIGHTS.exists():
         net = SEL.Mlp.load(SELECTOR_WEIGHTS)
-        f = SEL.features(L, info)
-        c = net.predict_class(f)
+        c = net.select(plan, L, info)  # best predicted class that applies to this matrix
         learned = {"class": c, "name": SEL.class_name(c), "time_over_best_fp64": float(times64[c] / times64[cls64])}
         net.close()
     sel64 = learned["class"] if learned else cls64
@@ -506,6 +557,170 @@ def run_ours(args, rank, world, local, dist):
     barrier(dist)
 
 
+# ------------------------------------------------------------ batched workload
+def batch_bytes(mats, ks) -> int:
+    return sum(algorithmic_bytes(m.n, m.nnz, k) for m, k in zip(mats, ks))
+
+
+def run_batch(args, rank, world, local, dist):
+    """The batched configuration: every system solved in one persistent launch
+    per solve (a CUDA graph replay); a step solves all 512 systems with all
+    their right-hand sides, so value = sum of right-hand sides / step time."""
+    import torch
+
+    import sptrsv_b200 as S
+    from oracle import oracle as O
+    from sptrsv_b200 import gen
+    from sptrsv_b200.batch import Batch
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    mats, ks, xs = gen.batch_config(512, seed=3)
+    bs = [m.matvec(x, k) for m, x, k in zip(mats, xs, ks)]
+    dev = [S.allocate_memory(m.rowptr, m.colidx, m.val, m.n) for m in mats]
+    t0 = time.perf_counter()
+    batch = Batch(dev, ks)
+    create_s = time.perf_counter() - t0
+    nk = sum(ks)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.empty_like(db)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        flush_buf.fill_(1)
+
+    refs = [O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k) for m, b, k in zip(mats, bs, ks)]
+
+    def max_err(xh):
+        return max(O.rel_err(xh[batch.offsets[s]:batch.offsets[s + 1]], refs[s]) for s in range(len(mats)))
+
+    # --- schedule: level-ordered vs hybrid, block size, refinement steps (exhaustive, small)
+    cands = []
+    for mode, width in ((0, 0.0), (2, 16.0)):
+        for bw in (8, 16):
+            cands.append((mode, width, bw))
+    res = {}
+    for mode, width, bw in cands:
+        batch.set_seq_width(width)
+        for prec, iters in ((64, 0), (32, 1), (32, 2)):
+            batch.set_schedule(mode=mode, block_warps=bw, ir_iters=iters)
+            t = statistics.median(event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), 3, 1, flush,
+                                                   stream))
+            S.sync_status()
+            res[(mode, width, bw, prec, iters)] = (t, max_err(dx.cpu().numpy()))
+    ok = {c: v for c, v in res.items() if v[1] <= TOL}
+    best = min(ok, key=lambda c: ok[c][0])
+    best64 = min((c for c in ok if c[3] == 64), key=lambda c: ok[c][0])
+    best32 = min((c for c in ok if c[3] == 32), key=lambda c: ok[c][0], default=None)
+
+    def apply(c):
+        mode, width, bw, prec, iters = c
+        batch.set_seq_width(width)
+        batch.set_schedule(mode=mode, block_warps=bw, ir_iters=iters)
+
+    apply(best)
+    prec = best[3]
+    sampler = ClockSampler(local)
+    barrier(dist)
+    torch.cuda.synchronize()
+    sampler.start()
+    ts = event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), args.steps, args.warmup, flush, stream)
+    clocks = sampler.stop()
+    torch.cuda.synchronize()
+    barrier(dist)
+    S.sync_status()
+    err = max_err(dx.cpu().numpy())
+    total_ms = reduce_max(dist, sum(ts))
+    ms_per_step = total_ms / args.steps
+    value = world * nk * args.steps / (total_ms / 1e3)
+    nseq, nseqw, nlvl = batch.seq_systems()
+
+    # plain FP64: the level-ordered batched launch, no sequential warps
+    batch.set_seq_width(0.0)
+    batch.set_schedule(mode=0, block_warps=8, ir_iters=1)
+    t_plain = statistics.median(event_time_steps(torch, lambda: batch.solve(db, dx, 64), max(3, args.steps // 2), 1,
+                                                 flush, stream))
+    S.sync_status()
+    err_plain = max_err(dx.cpu().numpy())
+    apply(best)
+
+    # roofline: one FP64 launch moves the compulsory bytes of every system
+    peak, peak_kind = measured_peak()
+    nbytes = batch_bytes(mats, ks)
+    c64 = best64
+    apply(c64)
+    t64 = statistics.median(event_time_steps(torch, lambda: batch.solve(db, dx, 64), max(3, args.steps // 2), 1, flush,
+                                             stream))
+    S.sync_status()
+    apply(best)
+    achieved = nbytes / (t64 / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": load_traffic("batch_f64_c3"), "kernel": "k_sptrsv_vk (one FP64 launch per solve)",
+                "algorithmic_bytes_per_launch": nbytes, "launch_ms": t64, "peak_kind": peak_kind,
+                "union_levels": batch.nlevs}
+
+    # end to end: pinned host b in, host x out, copies inside the timed region
+    hb = torch.from_numpy(np.concatenate(bs)).pin_memory()
+    hx = torch.empty(batch.vec_len, dtype=torch.float64).pin_memory()
+
+    def e2e():
+        db.copy_(hb, non_blocking=True)
+        batch.solve_graph(db, dx, prec)
+        hx.copy_(dx, non_blocking=True)
+
+    te = event_time_steps(torch, e2e, max(3, args.steps // 2), 1, flush, stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(dist, sum(te)) / len(te)
+    err_e2e = max_err(hx.numpy())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        done, t_cpu, sys_done = 0, 0.0, 0
+        for m, b, k in zip(mats, bs, ks):
+            _, dt = O.timed(O.solve, m.rowptr, m.colidx, m.val, b, k)
+            done += k
+            t_cpu += dt
+            sys_done += 1
+            if t_cpu > 10.0:
+                break
+        cpu = {"value": done / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"serial FP64 substitution of the first {sys_done} systems ({done} RHS, {t_cpu:.1f} s)"}
+    mode, width, bw, _, iters = best
+    line = {
+        "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == 64 else "f32+f64-refine", "data": "synthetic",
+        "config": {"workload": CONFIG_NAMES["c3"], "systems": len(mats), "n_total": batch.n,
+                   "nnz_total": int(sum(m.nnz for m in mats)), "rhs_total": nk, "nlevs_union": batch.nlevs,
+                   "l2": "flushed before every step (256 MiB write)",
+                   "schedule": {"mode": ["level", "chunk", "hybrid"][mode], "seq_width": width, "block_warps": bw,
+                                "ir_iters": iters, "sequential_systems": nseq, "sequential_warps": nseqw,
+                                "level_rows": nlvl},
+                   "selected_by": "exhaustive batch autotune", "parallelism": f"replicas x{world}"},
+        "gb_s": nbytes / (ms_per_step / 1e3) / 1e9, "hbm_frac": nbytes / (ms_per_step / 1e3) / 1e9 / peak,
+        "rel_err": {"tuned": err, "plain_fp64": err_plain, "e2e": err_e2e, "tol": TOL},
+        "autotune_ms": {f"{['level', 'chunk', 'hybrid'][c[0]]}/w{c[1]:g}/bw{c[2]}/p{c[3]}/ir{c[4]}": v[0]
+                        for c, v in res.items()},
+        "fp64_best_ms": res[best64][0],
+        "fp32_refine_best_ms": res[best32][0] if best32 else None,
+        "plain_fp64": {"solves_s": nk / (t_plain / 1e3), "ms": t_plain, "path": "level-ordered batched launch"},
+        "speedup_vs_plain_fp64": t_plain / ms_per_step,
+        "batch_create_s": create_s,
+        "e2e": {"value": world * nk / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * batch.vec_len,
+                "d2h_bytes_per_step": 8 * batch.vec_len},
+        "energy_j_per_solve": (clocks["power_w_mean"] * ms_per_step / 1e3 / nk
+                               if clocks and clocks.get("power_w_mean") else None),
+        "roofline": roofline, "gpu_launches": args.steps * (1 if prec == 64 else 1 + 2 * iters),
+        "clocks": clocks, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for d in dev:
+        S.free_device_analysis(d, None)
+    barrier(dist)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -525,6 +740,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world, dist)
+        elif args.config == "c3":
+            run_batch(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

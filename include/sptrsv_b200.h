@@ -203,12 +203,17 @@ typedef struct sptrsv_plan_s* sptrsv_plan_t;
 #define SPTRSV_VAR_MULTIROW  2  /* level order, lanes per row by row length          */
 #define SPTRSV_VAR_CLUSTER   3  /* level bands cut into row clusters, one CTA each;  */
                                 /* dependencies inside a cluster through shared mem  */
-#define SPTRSV_N_VARIANTS    4
+#define SPTRSV_VAR_STRIP     4  /* natural 32-row chunks whose inside dependencies   */
+                                /* are all on the previous row, solved by a prefix   */
+                                /* scan; rows_per_warp grid lines per warp (1..32),  */
+                                /* wavefront order; SPTRSV_ERR_UNSUPPORTED otherwise */
+#define SPTRSV_N_VARIANTS    5
 
 typedef struct {
     int variant;          /* SPTRSV_VAR_*                                            */
     int rows_per_warp;    /* 1,2,4,8,16,32: lanes per row = 32/rows_per_warp         */
-                          /* (MULTIROW takes lanes per row from the analysis map)     */
+                          /* (MULTIROW takes lanes per row from the analysis map;     */
+                          /* STRIP: chunk runs per warp)                              */
     int block_warps;      /* warps per CTA: 2, 4, 8 or 16                             */
     int warps_per_sm;     /* resident warps per SM of the persistent grid (0 = max)   */
     int backoff_ns;       /* nanosleep between polls after 8 failed polls (0 = spin)  */
@@ -290,12 +295,24 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
 int sptrsv_batch_destroy(sptrsv_batch_t batch);
 /* offsets[nsys+1] (may be NULL), total rows, levels of the union, packed length. */
 int sptrsv_batch_info(sptrsv_batch_t batch, long long* offsets, int* n_total, int* nlevs, long long* vec_len);
-/* chunked = 0 (default): level-ordered tasks over the union;
- * chunked = 1: each warp takes 32 consecutive rows of one system and solves
- * them in sequence, waiting once per chunk for the chunks it reads.
- * block_warps 2..16 (2..8 when chunked). */
-int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int chunked, int block_warps, int warps_per_sm,
+/* mode 0: level-ordered tasks over the union;
+ * mode 1: each warp takes 32 consecutive rows of one system and solves them
+ *         in sequence, waiting once per chunk for the chunks it reads;
+ * mode 2 (default): hybrid - every system with n_s / nlevs_s below the sequential
+ *         width (sptrsv_batch_set_seq_width) is solved by one warp in
+ *         natural order without waiting, the others by level-ordered tasks,
+ *         all in the same launch.
+ * block_warps 2..16 (2..8 in mode 1).  Rebuilds the level layout when the
+ * set of sequential systems changes. */
+int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int mode, int block_warps, int warps_per_sm,
                               int backoff_ns, int ir_iters);
+/* Width threshold of mode 2 (default 16): a system is sequential when
+ * n_s / nlevs_s < width and all its dependencies reach back at most
+ * 1024 / kp rows (kp = power of two >= its right-hand-side count); 0 makes
+ * no system sequential, >= 1e9 makes every system sequential. */
+int sptrsv_batch_set_seq_width(sptrsv_batch_t batch, double width);
+/* Systems solved sequentially, warps they occupy, rows left to the level tasks. */
+int sptrsv_batch_seq_systems(sptrsv_batch_t batch, int* nseq, int* nseq_warps, int* n_level_rows);
 /* b, x: DEVICE packed vectors; precision 64 plain FP64, 32 FP32 + FP64 refinement. */
 int sptrsv_batch_solve(sptrsv_batch_t batch, const double* b, double* x, int precision, cudaStream_t stream);
 /* Same solve captured once as a CUDA graph for these (b, x, precision) and

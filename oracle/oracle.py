@@ -44,7 +44,7 @@ def lib():
         L.oracle_n_warps.argtypes = [c_int, c_void_p]
         L.oracle_warp_map.restype = None
         L.oracle_warp_map.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
-        for f in ("oracle_solve_f64", "oracle_solve_ld", "oracle_spmv"):
+        for f in ("oracle_solve_f64", "oracle_solve_ld", "oracle_solve_f32", "oracle_spmv"):
             getattr(L, f).restype = None
             getattr(L, f).argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]
         L.oracle_solve_levels_omp.restype = None
@@ -91,12 +91,14 @@ def analysis(rowptr, colidx) -> dict:
             "n_warps": nw, "ibase_row": ibase, "ivect_size_warp": ivect[:nw], "warp_lev": wlev[:nw]}
 
 
-def solve(rowptr, colidx, val, b, nrhs: int = 1, long_double: bool = False) -> np.ndarray:
+def solve(rowptr, colidx, val, b, nrhs: int = 1, long_double: bool = False, f32: bool = False) -> np.ndarray:
+    """Serial substitution: FP64 (default), long double, or the reference's
+    FP32 build restated in float (f32)."""
     L = lib()
     rp, ci, va, bb = _i32(rowptr), _i32(colidx), _f64(val), _f64(b)
     n = rp.shape[0] - 1
     x = np.zeros(max(n * nrhs, 1), dtype=np.float64)
-    f = L.oracle_solve_ld if long_double else L.oracle_solve_f64
+    f = L.oracle_solve_ld if long_double else L.oracle_solve_f32 if f32 else L.oracle_solve_f64
     f(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, bb.ctypes.data, x.ctypes.data, nrhs)
     return x[: n * nrhs]
 
@@ -152,23 +154,13 @@ def mlp_gradient(params, mean, std, X, T, M):
 
 
 # ---- the reference's own kernels (GPU only; built by `make -C oracle ref`) ----
-REF32_SO = HERE / "_ref" / "libsptrsv_ref_f32.so"
-_r32 = None
+def ref_available() -> bool:
+    return REF_SO.exists()
 
 
-def ref_available(f32: bool = False) -> bool:
-    return (REF32_SO if f32 else REF_SO).exists()
-
-
-def ref_lib(f32: bool = False):
-    """The reference's kernels; f32 selects its VALUE_TYPE=float build (Makefile:7)."""
-    global _r, _r32
-    if f32:
-        if _r32 is None:
-            if not REF32_SO.exists():
-                raise FileNotFoundError(f"{REF32_SO} not built (make -C oracle ref32)")
-            _r32 = _bind_ref(ctypes.CDLL(str(REF32_SO)))
-        return _r32
+def ref_lib():
+    """The reference's FP64 kernels built from its sources (oracle/_ref)."""
+    global _r
     if _r is None:
         if not REF_SO.exists():
             raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref, needs the reference sources)")
@@ -209,10 +201,9 @@ def ref_analysis(rowptr, colidx, mode: int = 2) -> dict:
     return out
 
 
-def ref_solve(variant: int, rowptr, colidx, val, b, reps: int = 1, f32: bool = False):
-    """(x, median ms) of the reference solver 0 simple, 1 order, 2 multirow
-    (f32: its VALUE_TYPE=float build; values and b rounded to float)."""
-    L = ref_lib(f32)
+def ref_solve(variant: int, rowptr, colidx, val, b, reps: int = 1):
+    """(x, median ms) of the reference solver 0 simple, 1 order, 2 multirow."""
+    L = ref_lib()
     rp, ci, va, bb = _i32(rowptr), _i32(colidx), _f64(val), _f64(b)
     n = rp.shape[0] - 1
     x = np.zeros(n, dtype=np.float64)

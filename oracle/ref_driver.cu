@@ -116,7 +116,7 @@ static int upload(int n, const int* rowptr, const int* colidx, const double* val
     rp.push_back(rp[n]);
     std::vector<int> ci(colidx, colidx + nnz);
     ci.resize((size_t)nnz + 64, 0);
-    // values in the build's VALUE_TYPE (double, or float for the reference's FP32 build)
+    // values in the build's VALUE_TYPE (double, the reference's Makefile:7)
     std::vector<VALUE_TYPE> va((size_t)nnz + 64, (VALUE_TYPE)0);
     if (val) std::transform(val, val + nnz, va.begin(), [](double v) { return (VALUE_TYPE)v; });
     else std::fill(va.begin(), va.begin() + nnz, (VALUE_TYPE)1);

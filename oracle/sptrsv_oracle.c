@@ -161,6 +161,27 @@ void oracle_solve_f64(int n, const int* rowptr, const int* colidx, const double*
     }
 }
 
+/* The reference's FP32 build (VALUE_TYPE = float, Makefile:7) restated:
+ * values, b and x in float, piv = 1.0f / L_ii rounded in float, left_sum
+ * accumulated in float in column order (solve_csr_simple.cu:45,60-106 with
+ * VALUE_TYPE float).  x is returned widened to double. */
+void oracle_solve_f32(int n, const int* rowptr, const int* colidx, const double* val,
+                      const double* b, double* x, int nrhs)
+{
+    float* xf = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1) * (size_t)nrhs);
+    for (int i = 0; i < n; i++) {
+        int last = rowptr[i + 1] - 1;
+        float piv = 1.0f / (float)val[last];
+        for (int k = 0; k < nrhs; k++) {
+            float s = (float)b[(size_t)i * nrhs + k];
+            for (int p = rowptr[i]; p < last; p++) s -= (float)val[p] * xf[(size_t)colidx[p] * nrhs + k];
+            xf[(size_t)i * nrhs + k] = s * piv;
+        }
+    }
+    for (size_t t = 0; t < (size_t)n * nrhs; t++) x[t] = (double)xf[t];
+    free(xf);
+}
+
 /* The same substitution carried in long double, the cross-check of the FP64
  * oracle (x_i = (b_i - sum) / L_ii, exact division). */
 void oracle_solve_ld(int n, const int* rowptr, const int* colidx, const double* val,

@@ -27,8 +27,8 @@ SPTRSV_ERR_ALLOC = -7
 SPTRSV_ERR_NOT_CONVERGED = -8
 SPTRSV_ERR_UNSUPPORTED = -9
 
-VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER = 0, 1, 2, 3
-N_VARIANTS = 4
+VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER, VAR_STRIP = 0, 1, 2, 3, 4
+N_VARIANTS = 5
 
 
 class SpMat(ctypes.Structure):
@@ -109,6 +109,8 @@ _SIGS = {
     "sptrsv_batch_destroy": (c_int, [c_void_p]),
     "sptrsv_batch_info": (c_int, [c_void_p, c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong)]),
     "sptrsv_batch_set_schedule": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int]),
+    "sptrsv_batch_set_seq_width": (c_int, [c_void_p, c_double]),
+    "sptrsv_batch_seq_systems": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "sptrsv_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_batch_solve_graph": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_features": (c_int, [POINTER(SpMat), POINTER(AnalysisInfo), c_void_p]),

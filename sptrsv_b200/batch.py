@@ -27,9 +27,22 @@ class Batch:
         C.check(C.lib().sptrsv_batch_info(h, off.ctypes.data, byref(n), byref(nl), byref(vl)))
         self.offsets, self.n, self.nlevs, self.vec_len = off, n.value, nl.value, vl.value
 
-    def set_schedule(self, chunked: int = 0, block_warps: int = 8, warps_per_sm: int = 0, backoff_ns: int = 0,
+    LEVEL, CHUNK, HYBRID = 0, 1, 2
+
+    def set_schedule(self, mode: int = 2, block_warps: int = 8, warps_per_sm: int = 0, backoff_ns: int = 0,
                      ir_iters: int = 2):
-        C.check(C.lib().sptrsv_batch_set_schedule(self._h, chunked, block_warps, warps_per_sm, backoff_ns, ir_iters))
+        """mode 0 level-ordered, 1 natural-order chunks, 2 hybrid (near-chain
+        systems on one warp each, see set_seq_width)."""
+        C.check(C.lib().sptrsv_batch_set_schedule(self._h, mode, block_warps, warps_per_sm, backoff_ns, ir_iters))
+
+    def set_seq_width(self, width: float):
+        C.check(C.lib().sptrsv_batch_set_seq_width(self._h, float(width)))
+
+    def seq_systems(self) -> tuple[int, int, int]:
+        """(sequential systems, warps they occupy, rows left to the level tasks)."""
+        a, w, r = c_int(0), c_int(0), c_int(0)
+        C.check(C.lib().sptrsv_batch_seq_systems(self._h, byref(a), byref(w), byref(r)))
+        return a.value, w.value, r.value
 
     def solve(self, b, x, precision: int = 32, stream=None):
         C.check(C.lib().sptrsv_batch_solve(self._h, _dev(b, "float64", self.vec_len), _dev(x, "float64", self.vec_len),

@@ -11,6 +11,15 @@
 // systems advance together: a shallow system finishes early, a deep one
 // keeps a few warps busy to the end.
 //
+// A system whose levels hold few rows on average (n_s / nlevs_s below a
+// threshold; a near-chain) gains nothing from the level order: every level
+// costs a cross-warp hop through L2.  The hybrid schedule gives each such
+// system to one warp of the same persistent launch, which walks it in natural
+// order without any wait: the values of the most recent rows stay in a
+// shared-memory ring, older ones are re-read from x (written by the same
+// warp), and row metadata is loaded a chunk of 32 rows ahead.  The other
+// systems keep the level-ordered tasks on the remaining warps.
+//
 // Vectors are packed: system s owns the row-major n_s x k_s block starting at
 // element off_s (off_0 = 0, off_{s+1} = off_s + n_s k_s).  Each stored
 // off-diagonal entry keeps the packed offset of its column's row, so a wait
@@ -69,7 +78,21 @@ struct sptrsv_batch_s {
     int* flags = nullptr;        // [nchunks] chunk done flags (1 = done)
     int* row_sys = nullptr;      // [n] system of each union row
     int nchunks = 0;
-    int chunked = 0;             // 0: level-ordered tasks (default), 1: natural-order chunks
+    // per-system level structure and the hybrid schedule
+    int* lev = nullptr;          // [n] level of each union row (1-based)
+    int* d_kplog = nullptr;      // [nsys] log2 of the right-hand-side class
+    int* sys_task0 = nullptr;    // [nsys+1] first residual task of each system (32/kp rows per task)
+    int nres_tasks = 0;
+    std::vector<int> row0h;      // [nsys+1] first union row of each system
+    std::vector<int> sys_nlev;   // [nsys] levels of each system
+    std::vector<int> sys_dist;   // [nsys] largest row - column distance of an entry
+    std::vector<char> seq;       // [nsys] 1: solved by one warp in natural order (mode 2)
+    int n_lvl = 0;               // rows in the level layout (the non-sequential systems)
+    int* wptr = nullptr;         // [nseqw+1] per sequential warp: range in wsys
+    int* wsys = nullptr;         // systems in sequential-warp order
+    int nseqw = 0;
+    double seq_width = 16.0;     // mode 2: sequential when n_s / nlevs_s < seq_width
+    int mode = 2;                // 0: level-ordered tasks, 1: natural-order chunks, 2: hybrid
     int block_warps = 8, warps_per_sm = 0, backoff_ns = 0, ir_iters = 2;
     // graph cache for one (b, x, precision)
     cudaGraphExec_t gexec = nullptr;
@@ -90,17 +113,257 @@ struct BatchMat {
     const long long* __restrict__ xdep;
 };
 
-// variable right-hand-side count, one lane per (row, right-hand side)
+// Systems solved by one warp each (hybrid schedule), over the natural-order
+// union without diagonals.
+struct SeqSet {
+    const int* __restrict__ ptr;     // nptr
+    const int* __restrict__ col;     // ncol
+    const int* __restrict__ row0;    // [nsys+1]
+    const int* __restrict__ sk;      // [nsys]
+    const long long* __restrict__ soff;
+    const int* __restrict__ wptr;    // [nseqw+1]
+    const int* __restrict__ wsys;
+    int nseqw;
+};
+
+constexpr int kVkU = 8;         // elements per wait round in the level-ordered kernel
+constexpr int kSeqRing = 1024;  // ring elements per sequential warp
+constexpr int kSeqEC = 512;     // entries of one 32-row chunk that fit a stage buffer
+
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes_is8)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (bytes_is8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Shared memory of one sequential warp: the ring of recent x values, then
+// two stage buffers of one 32-row chunk each (relative row pointers, 1/diag,
+// columns, values, right-hand sides).
+template <typename V, typename T, typename BT>
+struct SeqSmem {
+    static constexpr size_t al(size_t x) { return (x + 15) & ~size_t(15); }
+    static constexpr size_t ring = al(kSeqRing * sizeof(T));
+    static constexpr size_t o_ptr = 0, o_di = al(33 * 4), o_col = o_di + al(32 * sizeof(V)),
+                            o_val = o_col + al(kSeqEC * 4), o_b = o_val + al(kSeqEC * sizeof(V)),
+                            buf = o_b + al(32 * 32 * sizeof(BT));
+    static constexpr size_t total = ring + 2 * buf;
+};
+
+// One warp solves system s in natural order without waiting on anyone.
+// Chunks of 32 rows are staged into shared memory with cp.async one chunk
+// ahead (their row pointers are loaded two chunks ahead), so a row's work
+// reads only shared memory: its entries, its right-hand sides and, for
+// columns at most rw rows back, the ring of recent x values (slot = row mod
+// rw).  An older column is read back from x, which this warp wrote.  Lane q
+// owns right-hand side q (K > 1, products subtracted in element order), or
+// the lanes stride a row's entries and reduce (K == 1).  A chunk with more
+// than kSeqEC entries is read from global memory instead.
 template <typename V, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(512) k_sptrsv_vk(BatchMat bm, const V* __restrict__ val, const V* __restrict__ di,
+__device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict__ val, const V* __restrict__ di,
+                                           int s, const BT* __restrict__ b, T* x, double* x64, unsigned char* region)
+{
+    using SM = SeqSmem<V, T, BT>;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int r0 = __ldg(q.row0 + s), r1 = __ldg(q.row0 + s + 1), K = __ldg(q.sk + s);
+    const long long off = __ldg(q.soff + s);
+    int kp = 1;
+    while (kp < K) kp <<= 1;
+    const int rw = kSeqRing / kp;
+    const bool lk = lane < K;
+    T* ring = reinterpret_cast<T*>(region);
+    auto bufp = [&](int bi) { return region + SM::ring + (size_t)bi * SM::buf; };
+    auto load_ptrs = [&](int cb, int& pl, int& pe) {
+        const int cnt = min(32, r1 - cb);
+        pl = lane < cnt ? __ldg(q.ptr + cb + lane) : 0;
+        pe = __ldg(q.ptr + cb + cnt);
+    };
+    // issues the copies of chunk cb into buffer bi; returns whether its entries fit
+    auto stage = [&](int bi, int cb, int pl, int pe, int& a_out) -> bool {
+        const int cnt = min(32, r1 - cb);
+        const int a = __shfl_sync(FULL, pl, 0);
+        const int E = pe - a;
+        unsigned char* base = bufp(bi);
+        int* sptr = reinterpret_cast<int*>(base + SM::o_ptr);
+        V* sdi = reinterpret_cast<V*>(base + SM::o_di);
+        int* scol = reinterpret_cast<int*>(base + SM::o_col);
+        V* sval = reinterpret_cast<V*>(base + SM::o_val);
+        BT* sb = reinterpret_cast<BT*>(base + SM::o_b);
+        if (lane < cnt) {
+            sptr[lane] = pl - a;
+            cp_async(sdi + lane, di + cb + lane, sizeof(V) == 8);
+        }
+        if (lane == 0) sptr[cnt] = E;
+        const bool fits = E <= kSeqEC;
+        if (fits)
+            for (int p = lane; p < E; p += 32) {
+                cp_async(scol + p, q.col + a + p, 0);
+                cp_async(sval + p, val + a + p, sizeof(V) == 8);
+            }
+        const long long bo = off + (long long)(cb - r0) * K;
+        for (int p = lane; p < cnt * K; p += 32) cp_async(sb + p, b + bo + p, sizeof(BT) == 8);
+        cp_async_commit();
+        a_out = a;
+        return fits;
+    };
+    int pl1 = 0, pe1 = 0, a_cur = 0, a_next = 0;
+    load_ptrs(r0, pl1, pe1);
+    bool fit_cur = stage(0, r0, pl1, pe1, a_cur);
+    if (r0 + 32 < r1) load_ptrs(r0 + 32, pl1, pe1);
+    cp_async_wait_all();
+    __syncwarp();
+    for (int c = 0, cb = r0; cb < r1; c++, cb += 32) {
+        const int bi = c & 1;
+        const int cnt = min(32, r1 - cb);
+        bool fit_next = true;
+        if (cb + 32 < r1) {
+            fit_next = stage(bi ^ 1, cb + 32, pl1, pe1, a_next);
+            if (cb + 64 < r1) load_ptrs(cb + 64, pl1, pe1);
+        }
+        const unsigned char* base = bufp(bi);
+        const int* __restrict__ sptr = reinterpret_cast<const int*>(base + SM::o_ptr);
+        const V* __restrict__ sdi = reinterpret_cast<const V*>(base + SM::o_di);
+        const int* __restrict__ scol = reinterpret_cast<const int*>(base + SM::o_col);
+        const V* __restrict__ sval = reinterpret_cast<const V*>(base + SM::o_val);
+        const BT* __restrict__ sb = reinterpret_cast<const BT*>(base + SM::o_b);
+        const int* gcol = q.col + a_cur;
+        const V* gval = val + a_cur;
+        if (K == 1) {
+            // lane j owns row cb + j: first the entries before the chunk
+            // (final values, a sorted prefix of the row), then a sweep over
+            // the chunk in which row t's value is broadcast and every later
+            // row holding column cb + t subtracts its product
+            const int j = lane, i = cb + j;
+            const bool own = j < cnt;
+            T acc = own ? (T)sb[j] : (T)0;
+            const T piv = own ? (T)sdi[j] : (T)0;
+            int p = own ? sptr[j] : 0;
+            const int pe = own ? sptr[j + 1] : 0;
+            int nc = 0x7fffffff;
+            T nv = 0;
+            for (; p < pe; p++) {
+                const int cc = fit_cur ? scol[p] : __ldg(gcol + p);
+                const T vv = (T)(fit_cur ? sval[p] : __ldg(gval + p));
+                if (cc >= cb) {
+                    nc = cc;
+                    nv = vv;
+                    break;
+                }
+                acc -= vv * ((i - cc <= rw) ? ring[cc & (rw - 1)] : __ldcg(x + off + (cc - r0)));
+            }
+            T res = 0;
+            for (int t = 0; t < cnt; t++) {
+                const T mine = publishable(acc * piv);
+                const T xt = __shfl_sync(FULL, mine, t);
+                if (j == t) res = xt;
+                if (nc == cb + t) {
+                    acc -= nv * xt;
+                    nc = 0x7fffffff;
+                    if (++p < pe) {
+                        nc = fit_cur ? scol[p] : __ldg(gcol + p);
+                        nv = (T)(fit_cur ? sval[p] : __ldg(gval + p));
+                    }
+                }
+            }
+            if (own) {
+                ring[i & (rw - 1)] = res;
+                const long long xi = off + (i - r0);
+                x[xi] = res;
+                if (OUT == 1) x64[xi] = (double)res;
+                if (OUT == 2) x64[xi] += (double)res;
+            }
+        } else {
+            // lane q owns right-hand side q; rows one after another.  A row's
+            // columns more than rw rows back (a sorted prefix, usually empty)
+            // are read from x, the rest from the ring without a branch, four
+            // at a time so their loads overlap.  The next row's pointers,
+            // 1/diag and right-hand side are read one row ahead.
+            if (lk) {
+                T* __restrict__ rl = ring + lane;
+                int e0 = sptr[0], e1 = sptr[1];
+                T piv = (T)sdi[0], bj = (T)sb[lane];
+                for (int j = 0; j < cnt; j++) {
+                    const int i = cb + j;
+                    int ne1 = 0;
+                    T npiv = 0, nbj = 0;
+                    if (j + 1 < cnt) {
+                        ne1 = sptr[j + 2];
+                        npiv = (T)sdi[j + 1];
+                        nbj = (T)sb[(j + 1) * K + lane];
+                    }
+                    T acc = bj;
+                    int p = e0;
+                    if (fit_cur) {
+                        for (; p < e1; p++) {  // columns beyond the ring
+                            const int cc = scol[p];
+                            if (i - cc <= rw) break;
+                            acc -= (T)sval[p] * __ldcg(x + off + (long long)(cc - r0) * K + lane);
+                        }
+                        const int msk = rw - 1;
+                        for (; p + 4 <= e1; p += 4) {
+                            const int c0 = scol[p], c1 = scol[p + 1], c2 = scol[p + 2], c3 = scol[p + 3];
+                            const T v0 = (T)sval[p], v1 = (T)sval[p + 1], v2 = (T)sval[p + 2], v3 = (T)sval[p + 3];
+                            const T x0 = rl[(c0 & msk) * kp], x1 = rl[(c1 & msk) * kp], x2 = rl[(c2 & msk) * kp],
+                                    x3 = rl[(c3 & msk) * kp];
+                            acc -= v0 * x0;
+                            acc -= v1 * x1;
+                            acc -= v2 * x2;
+                            acc -= v3 * x3;
+                        }
+                        for (; p < e1; p++) acc -= (T)sval[p] * rl[(scol[p] & msk) * kp];
+                    } else {
+                        for (; p < e1; p++) {
+                            const int cc = __ldg(gcol + p);
+                            const T xc = (i - cc <= rw) ? rl[(cc & (rw - 1)) * kp]
+                                                        : __ldcg(x + off + (long long)(cc - r0) * K + lane);
+                            acc -= (T)__ldg(gval + p) * xc;
+                        }
+                    }
+                    const T res = publishable(acc * piv);
+                    rl[(i & (rw - 1)) * kp] = res;
+                    const long long xi = off + (long long)(i - r0) * K + lane;
+                    x[xi] = res;
+                    if (OUT == 1) x64[xi] = (double)res;
+                    if (OUT == 2) x64[xi] += (double)res;
+                    e0 = e1;
+                    e1 = ne1;
+                    piv = npiv;
+                    bj = nbj;
+                }
+            }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        fit_cur = fit_next;
+        a_cur = a_next;
+    }
+}
+
+// Variable right-hand-side count, one lane per (row, right-hand side), over
+// level-aligned tasks.  With sequential systems (q.nseqw > 0) the warps are
+// numbered w = (warp in block) * gridDim + block; w < nseqw runs its
+// sequential systems, the others take the level tasks round-robin.
+template <typename V, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(512, 1) k_sptrsv_vk(BatchMat bm, const V* __restrict__ val, const V* __restrict__ di,
                                                    int ntasks, const int* __restrict__ tbase,
-                                                   const int* __restrict__ tkp, const BT* __restrict__ b, T* x,
+                                                   const int* __restrict__ tkp, SeqSet q, const V* __restrict__ nval,
+                                                   const V* __restrict__ ndi, const BT* __restrict__ b, T* x,
                                                    double* x64, DevStatus* st, unsigned long long budget,
                                                    unsigned backoff)
 {
-    const int lane = threadIdx.x & 31;
-    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int w = wib * (int)gridDim.x + (int)blockIdx.x;
+    if (w < q.nseqw) {  // w < nseqw implies wib == 0: one sequential warp per block
+        for (int z = __ldg(q.wptr + w); z < __ldg(q.wptr + w + 1); z++)
+            seq_system<V, T, BT, OUT>(q, nval, ndi, __ldg(q.wsys + z), b, x, x64, smem_raw);
+        return;
+    }
+    const int gw = w - q.nseqw;
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5) - q.nseqw;
     for (int t = gw; t < ntasks; t += nw) {
         const int base = __ldg(tbase + t), cnt = __ldg(tbase + t + 1) - base, kp = __ldg(tkp + t);
         const int seg = lane / kp, k = lane & (kp - 1);
@@ -116,18 +379,26 @@ __global__ void __launch_bounds__(512) k_sptrsv_vk(BatchMat bm, const V* __restr
             s = __ldg(bm.ptr + pos);
             len = __ldg(bm.ptr + pos + 1) - s;
         }
-        // rows of a task are in one level: the warp waits for each round together
+        // rows of a task are in one level: the warp waits for each round of
+        // kVkU elements together (loads issued back to back)
         const int rounds = __reduce_max_sync(0xffffffffu, len);
-        for (int j = 0; j < rounds; j++) {
-            const bool have = j < len;
-            long long xc = 0;
-            T v = 0, xv = 0;
-            if (have) {
-                xc = __ldg(bm.xdep + s + j);
-                v = (T)__ldg(val + s + j);
+        for (int j = 0; j < rounds; j += kVkU) {
+            const int nh = min(kVkU, len - j);
+            long long xc[kVkU];
+            T vv[kVkU], xv[kVkU];
+#pragma unroll
+            for (int u = 0; u < kVkU; u++) {
+                xc[u] = 0;
+                vv[u] = 0;
+                if (u < nh) {
+                    xc[u] = __ldg(bm.xdep + s + j + u) + k;
+                    vv[u] = (T)__ldg(val + s + j + u);
+                }
             }
-            if (!warp_wait<false, T>(have, 0, x + xc + k, nullptr, xv, st, budget, backoff, pos)) return;
-            if (have) acc -= v * xv;
+            if (!warp_wait_n<false, kVkU, T>(nh, xc, x, nullptr, xv, st, budget, backoff, pos)) return;
+#pragma unroll
+            for (int u = 0; u < kVkU; u++)
+                if (u < nh) acc -= vv[u] * xv[u];
         }
         if (act) {
             T r = publishable(acc * piv);
@@ -218,47 +489,49 @@ __global__ void __launch_bounds__(256) k_sptrsv_vkc(NatBatch nb, const V* __rest
     }
 }
 
-// r = b - L x in FP64 over the natural-order union, one warp per row, lanes over the right-hand sides
-__global__ void __launch_bounds__(256) k_residual_vkc(const int* __restrict__ ptr, const int* __restrict__ col,
+// r = b - L x in FP64 over the natural-order union (no dependencies).  Warp
+// task t covers 32/kp consecutive rows of one system (kp lanes per row, lane
+// k of a row owns right-hand side k); sys_task0[s] is the first task of
+// system s.  Elements are taken four at a time so their loads overlap.
+__global__ void __launch_bounds__(256) k_residual_nat(const int* __restrict__ ptr, const int* __restrict__ col,
                                                       const double* __restrict__ val, const double* __restrict__ dg,
-                                                      const int* __restrict__ row_sys, const int* __restrict__ row0,
-                                                      const int* __restrict__ sk, const long long* __restrict__ soff,
-                                                      int n, const double* __restrict__ b,
+                                                      const int* __restrict__ sys_task0, int nsys,
+                                                      const int* __restrict__ row0, const int* __restrict__ sk,
+                                                      const int* __restrict__ kplog,
+                                                      const long long* __restrict__ soff, const double* __restrict__ b,
                                                       const double* __restrict__ x, float* __restrict__ r)
 {
     const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-        const int s = row_sys[i], K = sk[s], r0 = row0[s];
-        if (lane >= K) continue;
-        const long long o = soff[s];
-        const long long xr = o + (long long)(i - r0) * K + lane;
+    const int ntask = __ldg(sys_task0 + nsys);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    for (int t = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); t < ntask; t += nw) {
+        int lo = 0, hi = nsys - 1;  // system: largest s with sys_task0[s] <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(sys_task0 + mid) <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const int s = lo, lg = __ldg(kplog + s), K = __ldg(sk + s), r0 = __ldg(row0 + s);
+        const int k = lane & ((1 << lg) - 1);
+        const int i = r0 + ((t - __ldg(sys_task0 + s)) << (5 - lg)) + (lane >> lg);
+        if (i >= __ldg(row0 + s + 1) || k >= K) continue;
+        const long long xb = soff[s] + k - (long long)r0 * K;  // x[xb + c * K]: row c, right-hand side k
+        const long long xr = xb + (long long)i * K;
         double acc = b[xr] - dg[i] * x[xr];
-        for (int p = ptr[i]; p < ptr[i + 1]; p++) acc -= val[p] * x[o + (long long)(col[p] - r0) * K + lane];
+        int p = ptr[i];
+        const int e = ptr[i + 1];
+        for (; p + 4 <= e; p += 4) {
+            const int c0 = col[p], c1 = col[p + 1], c2 = col[p + 2], c3 = col[p + 3];
+            const double v0 = val[p], v1 = val[p + 1], v2 = val[p + 2], v3 = val[p + 3];
+            const double x0 = x[xb + (long long)c0 * K], x1 = x[xb + (long long)c1 * K],
+                         x2 = x[xb + (long long)c2 * K], x3 = x[xb + (long long)c3 * K];
+            acc -= v0 * x0;
+            acc -= v1 * x1;
+            acc -= v2 * x2;
+            acc -= v3 * x3;
+        }
+        for (; p < e; p++) acc -= val[p] * x[xb + (long long)col[p] * K];
         r[xr] = (float)acc;
-    }
-}
-
-// r = b - L x in FP64 over the batch layout (no dependencies)
-__global__ void __launch_bounds__(256) k_residual_vk(BatchMat bm, const double* __restrict__ val,
-                                                     const double* __restrict__ dg, int ntasks,
-                                                     const int* __restrict__ tbase, const int* __restrict__ tkp,
-                                                     const double* __restrict__ b, const double* __restrict__ x,
-                                                     float* __restrict__ r)
-{
-    const int lane = threadIdx.x & 31;
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long t = gw; t < ntasks; t += nw) {
-        const int base = tbase[t], cnt = tbase[t + 1] - base, kp = tkp[t];
-        const int seg = lane / kp, k = lane & (kp - 1);
-        if (seg >= cnt) continue;
-        const int pos = base + seg;
-        if (k >= bm.krow[pos]) continue;
-        const long long xr = bm.xrow[pos];
-        double acc = b[xr + k] - dg[pos] * x[xr + k];
-        for (int p = bm.ptr[pos]; p < bm.ptr[pos + 1]; p++) acc -= val[p] * x[bm.xdep[p] + k];
-        r[xr + k] = (float)acc;
     }
 }
 
@@ -273,60 +546,105 @@ __global__ void k_union_cols(const int* __restrict__ ci, int nnz_s, int row0, in
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz_s; i += gridDim.x * blockDim.x) uci[i] = ci[i] + row0;
 }
 
-// key = (level-1)*6 + log2(kp) per union row; row data for the layout
+// key = (level-1)*6 + log2(kp) per union row; rows of sequential systems get
+// the key 6*nlevs, past every level, so they sort to the end of the layout
 __global__ void k_batch_keys(const int* __restrict__ level, const int* __restrict__ sys_of_row,
-                             const int* __restrict__ kp_log, int n, int* __restrict__ key, int* __restrict__ iota)
+                             const int* __restrict__ kp_log, const int* __restrict__ seqf, int nlevs, int n,
+                             int* __restrict__ key, int* __restrict__ iota)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        key[i] = (level[i] - 1) * 6 + kp_log[sys_of_row[i]];
+        const int s = sys_of_row[i];
+        key[i] = seqf[s] ? 6 * nlevs : (level[i] - 1) * 6 + kp_log[s];
         iota[i] = i;
     }
 }
 
-__global__ void k_batch_rows(const int* __restrict__ order, const int* __restrict__ urp, int n,
-                             int* __restrict__ len, int* __restrict__ pos_of)
+__global__ void k_batch_rows(const int* __restrict__ order, const int* __restrict__ nptr, int n_lvl,
+                             int* __restrict__ len)
 {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x) {
-        if (p == n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n_lvl; p += gridDim.x * blockDim.x) {
+        if (p == n_lvl) {
             len[p] = 0;
             continue;
         }
-        int r = order[p];
-        pos_of[r] = p;
-        len[p] = urp[r + 1] - urp[r] - 1;
+        const int r = order[p];
+        len[p] = nptr[r + 1] - nptr[r];
     }
 }
 
-__global__ void k_batch_fill(const int* __restrict__ order, const int* __restrict__ urp, const int* __restrict__ uci,
-                             const double* __restrict__ uva, const int* __restrict__ sys_of_row,
-                             const int* __restrict__ row0, const long long* __restrict__ soff,
-                             const int* __restrict__ sk, const int* __restrict__ ptr, int n, long long* __restrict__ xrow,
+// level layout positions p < n_lvl from the natural-order union
+__global__ void k_batch_fill(const int* __restrict__ order, const int* __restrict__ nptr, const int* __restrict__ ncol,
+                             const double* __restrict__ nval, const double* __restrict__ ndg,
+                             const int* __restrict__ sys_of_row, const int* __restrict__ row0,
+                             const long long* __restrict__ soff, const int* __restrict__ sk,
+                             const int* __restrict__ ptr, int n_lvl, long long* __restrict__ xrow,
                              int* __restrict__ krow, long long* __restrict__ xdep, double* __restrict__ val64,
                              float* __restrict__ val32, double* __restrict__ dg64, double* __restrict__ di64,
                              float* __restrict__ di32)
 {
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n; p += nw) {
+    for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_lvl; p += nw) {
         const int r = order[p];
         const int s = sys_of_row[r];
         const long long o = soff[s];
         const int k = sk[s], r0 = row0[s];
-        const int a = urp[r], e = urp[r + 1] - 1, dst = ptr[p];
+        const int a = nptr[r], e = nptr[r + 1], dst = ptr[p];
         for (int q = a + lane; q < e; q += 32) {
-            const int c = uci[q];
+            const int c = ncol[q];
             xdep[dst + q - a] = o + (long long)(c - r0) * k;
-            val64[dst + q - a] = uva[q];
-            val32[dst + q - a] = (float)uva[q];
+            val64[dst + q - a] = nval[q];
+            val32[dst + q - a] = (float)nval[q];
         }
         if (lane == 0) {
-            const double d = uva[e];
+            const double d = ndg[r];
             xrow[p] = o + (long long)(r - r0) * k;
             krow[p] = k;
             dg64[p] = d;
             di64[p] = 1.0 / d;
             di32[p] = 1.0f / (float)d;
         }
+    }
+}
+
+// largest row - column distance of each system (the first entry of a row has
+// its smallest column; one block per system)
+__global__ void k_sys_dist(const int* __restrict__ nptr, const int* __restrict__ ncol, const int* __restrict__ row0,
+                           int nsys, int* __restrict__ out)
+{
+    __shared__ int red[32];
+    for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+        int m = 0;
+        for (int i = row0[s] + threadIdx.x; i < row0[s + 1]; i += blockDim.x)
+            if (nptr[i + 1] > nptr[i]) m = max(m, i - ncol[nptr[i]]);
+        m = __reduce_max_sync(0xffffffffu, m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+            v = __reduce_max_sync(0xffffffffu, v);
+            if (threadIdx.x == 0) out[s] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// levels of each system: the largest level among its rows (one block per system)
+__global__ void k_sys_nlevs(const int* __restrict__ lev, const int* __restrict__ row0, int nsys, int* __restrict__ out)
+{
+    __shared__ int red[32];
+    for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+        int m = 0;
+        for (int i = row0[s] + threadIdx.x; i < row0[s + 1]; i += blockDim.x) m = max(m, lev[i]);
+        m = __reduce_max_sync(0xffffffffu, m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+            v = __reduce_max_sync(0xffffffffu, v);
+            if (threadIdx.x == 0) out[s] = v;
+        }
+        __syncthreads();
     }
 }
 
@@ -391,17 +709,19 @@ void batch_free(sptrsv_batch_s* B)
     cudaFree(B->nptr); cudaFree(B->ncol); cudaFree(B->nval64); cudaFree(B->nval32); cudaFree(B->ndg64);
     cudaFree(B->ndi64); cudaFree(B->ndi32); cudaFree(B->tsys); cudaFree(B->tj); cudaFree(B->cdep);
     cudaFree(B->sys_row0); cudaFree(B->sys_chunk0); cudaFree(B->sys_k); cudaFree(B->sys_off); cudaFree(B->flags);
-    cudaFree(B->row_sys);
+    cudaFree(B->row_sys); cudaFree(B->lev); cudaFree(B->d_kplog); cudaFree(B->wptr); cudaFree(B->wsys);
+    cudaFree(B->sys_task0);
     cudaFree(B->ptr); cudaFree(B->xrow); cudaFree(B->krow); cudaFree(B->xdep); cudaFree(B->val64);
     cudaFree(B->val32); cudaFree(B->dg64); cudaFree(B->di64); cudaFree(B->di32); cudaFree(B->tbase);
     cudaFree(B->tkp); cudaFree(B->w32a); cudaFree(B->w32b);
 }
 
-// Level- and class-aligned tasks: a segment is one (level, kp) key and is
-// cut into tasks of 32/kp rows; tkp[t] = kp of the task's segment.
+// Level- and class-aligned tasks over the first n_lvl layout positions: a
+// segment is one (level, kp) key and is cut into tasks of 32/kp rows;
+// tkp[t] = kp of the task's segment.
 int batch_tasks(sptrsv_batch_s* B, const int* key_sorted, int K, cudaStream_t s)
 {
-    int e = build_task_table(key_sorted, B->n, K, 0, &B->tbase, &B->ntasks, s);
+    int e = build_task_table(key_sorted, B->n_lvl, K, 0, &B->tbase, &B->ntasks, s);
     if (e) return e;
     SPT_CUDA(dalloc(&B->tkp, B->ntasks));
     if (B->ntasks > 0) {
@@ -411,13 +731,176 @@ int batch_tasks(sptrsv_batch_s* B, const int* key_sorted, int K, cudaStream_t s)
     return 0;
 }
 
+// (Re)builds the level layout for the systems not marked sequential in
+// B->seq: order (level, rhs class), stable in the natural order.
+int batch_level_layout(sptrsv_batch_s* B, cudaStream_t s)
+{
+    int** ip[] = {&B->ptr, &B->krow, &B->tbase, &B->tkp};
+    for (int** p : ip) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    cudaFree(B->xrow); cudaFree(B->xdep); cudaFree(B->val64); cudaFree(B->val32); cudaFree(B->dg64);
+    cudaFree(B->di64); cudaFree(B->di32);
+    B->xrow = B->xdep = nullptr;
+    B->val64 = B->dg64 = B->di64 = nullptr;
+    B->val32 = B->di32 = nullptr;
+    B->ntasks = 0;
+    const long long n = B->n;
+    long long n_lvl = 0, m_lvl = 0;  // m_lvl: read back from the row pointer scan
+    for (int k = 0; k < B->nsys; k++)
+        if (!B->seq[k]) n_lvl += B->row0h[k + 1] - B->row0h[k];
+    B->n_lvl = (int)n_lvl;
+    int *d_seq = nullptr, *key = nullptr, *ord = nullptr, *kt = nullptr, *vt = nullptr, *scr = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_seq); cudaFree(key); cudaFree(ord); cudaFree(kt); cudaFree(vt); cudaFree(scr);
+    };
+#define LCHK(call)                            \
+    do {                                      \
+        cudaError_t e_ = (call);              \
+        if (e_ != cudaSuccess) {              \
+            cleanup();                        \
+            return cuda_fail(e_, #call);      \
+        }                                     \
+    } while (0)
+    std::vector<int> seqi(B->seq.begin(), B->seq.end());
+    LCHK(dalloc(&d_seq, B->nsys));
+    LCHK(cudaMemcpy(d_seq, seqi.data(), sizeof(int) * (size_t)B->nsys, cudaMemcpyHostToDevice));
+    LCHK(dalloc(&key, n));
+    LCHK(dalloc(&ord, n));
+    LCHK(dalloc(&kt, n));
+    LCHK(dalloc(&vt, n));
+    const long long sc1 = radix_scratch_ints(n), sc2 = scan_scratch_ints(n + 1);
+    LCHK(dalloc(&scr, sc1 > sc2 ? sc1 : sc2));
+    k_batch_keys<<<grid_for(n, 256), 256, 0, s>>>(B->lev, B->row_sys, B->d_kplog, d_seq, B->nlevs, (int)n, key, ord);
+    LCHK(cudaGetLastError());
+    LCHK(radix_sort_pairs(key, ord, kt, vt, n, 6 * B->nlevs, scr, s));
+    LCHK(dalloc(&B->ptr, n_lvl + 1));
+    k_batch_rows<<<grid_for(n_lvl + 1, 256), 256, 0, s>>>(ord, B->nptr, (int)n_lvl, B->ptr);
+    LCHK(cudaGetLastError());
+    LCHK(scan_exclusive(B->ptr, B->ptr, n_lvl + 1, scr, s));
+    int mm = 0;
+    LCHK(cudaMemcpyAsync(&mm, B->ptr + n_lvl, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LCHK(cudaStreamSynchronize(s));
+    m_lvl = mm;
+    LCHK(dalloc(&B->xrow, n_lvl));
+    LCHK(dalloc(&B->krow, n_lvl));
+    LCHK(dalloc(&B->xdep, m_lvl));
+    LCHK(dalloc(&B->val64, m_lvl));
+    LCHK(dalloc(&B->val32, m_lvl));
+    LCHK(dalloc(&B->dg64, n_lvl));
+    LCHK(dalloc(&B->di64, n_lvl));
+    LCHK(dalloc(&B->di32, n_lvl));
+    if (n_lvl > 0) {
+        k_batch_fill<<<grid_for(n_lvl * 32, 256), 256, 0, s>>>(ord, B->nptr, B->ncol, B->nval64, B->ndg64,
+                                                                B->row_sys, B->sys_row0, B->sys_off, B->sys_k,
+                                                                B->ptr, (int)n_lvl, B->xrow, B->krow, B->xdep,
+                                                                B->val64, B->val32, B->dg64, B->di64, B->di32);
+        LCHK(cudaGetLastError());
+    }
+    {
+        int e = batch_tasks(B, key, 6 * B->nlevs, s);
+        if (e) {
+            cleanup();
+            return e;
+        }
+    }
+    LCHK(cudaStreamSynchronize(s));
+#undef LCHK
+    cleanup();
+    return 0;
+}
+
+constexpr int kModeLevel = 0, kModeChunk = 1, kModeHybrid = 2;
+constexpr double kSeqAll = 1e9;  // a sequential width this large makes every system sequential
+
+
+// The level-ordered launch's grid size (every instantiation that a solve
+// launches), before any sequential-warp assignment.
+template <typename V, typename T, typename BT, int OUT>
+int vk_grid(const sptrsv_batch_s* B, long long max_blocks, long long* g)
+{
+    const int cap = B->warps_per_sm > 0 ? (B->warps_per_sm + B->block_warps - 1) / B->block_warps : 0;
+    const size_t smem = SeqSmem<V, T, BT>::total;
+    SPT_CUDA(persistent_grid(k_sptrsv_vk<V, T, BT, OUT>, 32 * B->block_warps, smem, max_blocks, cap, g));
+    return 0;
+}
+
+long long vk_max_blocks(const sptrsv_batch_s* B, int nseqw)
+{
+    const long long a = div_up(B->ntasks, B->block_warps), c = nseqw;
+    return std::max(std::max(a, c), 1LL);
+}
+
+// Marks the sequential systems (mode 2: n_s / nlevs_s < seq_width and every
+// dependency within the ring window of the system's right-hand-side class,
+// or every system when seq_width >= kSeqAll), rebuilds the level layout when
+// the set changed, and spreads the sequential systems
+// over at most one warp per block of the grid, largest first, each to the warp
+// with the least work so far.
+int batch_apply_schedule(sptrsv_batch_s* B, cudaStream_t s)
+{
+    std::vector<char> seq(B->nsys, 0);
+    if (B->mode == kModeHybrid)
+        for (int k = 0; k < B->nsys; k++) {
+            const double nk = B->row0h[k + 1] - B->row0h[k];
+            int kp = 1;
+            while (kp < B->kk[k]) kp <<= 1;
+            const bool fits = B->sys_dist[k] <= kSeqRing / kp;
+            seq[k] = B->seq_width >= kSeqAll || (fits && nk < B->seq_width * std::max(1, B->sys_nlev[k]));
+        }
+    if (seq != B->seq || !B->ptr) {
+        B->seq = seq;
+        int e = batch_level_layout(B, s);
+        if (e) return e;
+    }
+    std::vector<int> list;
+    for (int k = 0; k < B->nsys; k++)
+        if (B->seq[k]) list.push_back(k);
+    cudaFree(B->wptr);
+    cudaFree(B->wsys);
+    B->wptr = B->wsys = nullptr;
+    B->nseqw = 0;
+    if (list.empty()) return 0;
+    long long g = 0, gmin = 1LL << 40;
+    const long long mb = vk_max_blocks(B, (int)list.size());
+    int e = vk_grid<double, double, double, 0>(B, mb, &g);
+    if (e) return e;
+    gmin = std::min(gmin, g);
+    if ((e = vk_grid<float, float, double, 1>(B, mb, &g))) return e;
+    gmin = std::min(gmin, g);
+    if ((e = vk_grid<float, float, float, 2>(B, mb, &g))) return e;
+    gmin = std::min(gmin, g);
+    const int nw = (int)std::min<long long>((long long)list.size(), gmin);
+    auto work = [&](int k) { return (double)(B->row0h[k + 1] - B->row0h[k]) * (1.0 + B->kk[k] / 8.0); };
+    std::stable_sort(list.begin(), list.end(), [&](int a, int b2) { return work(a) > work(b2); });
+    std::vector<std::vector<int>> per(nw);
+    std::vector<double> load(nw, 0.0);
+    for (int k : list) {
+        const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        per[w].push_back(k);
+        load[w] += work(k);
+    }
+    std::vector<int> wp(nw + 1, 0), ws;
+    for (int w = 0; w < nw; w++) {
+        ws.insert(ws.end(), per[w].begin(), per[w].end());
+        wp[w + 1] = (int)ws.size();
+    }
+    SPT_CUDA(dalloc(&B->wptr, nw + 1));
+    SPT_CUDA(dalloc(&B->wsys, (long long)ws.size()));
+    SPT_CUDA(cudaMemcpy(B->wptr, wp.data(), sizeof(int) * wp.size(), cudaMemcpyHostToDevice));
+    SPT_CUDA(cudaMemcpy(B->wsys, ws.data(), sizeof(int) * ws.size(), cudaMemcpyHostToDevice));
+    B->nseqw = nw;
+    return 0;
+}
+
 template <typename V, typename T, typename BT, int OUT>
 int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cudaStream_t s)
 {
     Ctx* c = ctx();
     const int block = 32 * B->block_warps;
     const int cap = B->warps_per_sm > 0 ? (B->warps_per_sm + B->block_warps - 1) / B->block_warps : 0;
-    if (B->chunked) {
+    if (B->mode == kModeChunk) {
         const V* val = f32 ? reinterpret_cast<const V*>(B->nval32) : reinterpret_cast<const V*>(B->nval64);
         const V* di = f32 ? reinterpret_cast<const V*>(B->ndi32) : reinterpret_cast<const V*>(B->ndi64);
         NatBatch nb{B->nptr, B->ncol, B->tsys, B->tj, B->cdep, B->sys_row0, B->sys_chunk0, B->sys_k, B->sys_off};
@@ -433,25 +916,26 @@ int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cu
     }
     const V* val = f32 ? reinterpret_cast<const V*>(B->val32) : reinterpret_cast<const V*>(B->val64);
     const V* di = f32 ? reinterpret_cast<const V*>(B->di32) : reinterpret_cast<const V*>(B->di64);
+    const V* nval = f32 ? reinterpret_cast<const V*>(B->nval32) : reinterpret_cast<const V*>(B->nval64);
+    const V* ndi = f32 ? reinterpret_cast<const V*>(B->ndi32) : reinterpret_cast<const V*>(B->ndi64);
     BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
+    SeqSet q{B->nptr, B->ncol, B->sys_row0, B->sys_k, B->sys_off, B->wptr, B->wsys, B->nseqw};
     auto kern = k_sptrsv_vk<V, T, BT, OUT>;
-    SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(B->ntasks, B->block_warps), cap, s, bm, val, di,
-                                      B->ntasks, (const int*)B->tbase, (const int*)B->tkp, b, x, x64, c->d_status,
-                                      wait_budget_ns(), (unsigned)B->backoff_ns));
+    const size_t smem = B->nseqw > 0 ? SeqSmem<V, T, BT>::total : 0;
+    if (smem > 48 * 1024)
+        SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (B->ntasks == 0 && B->nseqw == 0) return 0;
+    SPT_CUDA(launch_persistent_capped(kern, block, smem, vk_max_blocks(B, B->nseqw), cap, s, bm, val, di, B->ntasks,
+                                      (const int*)B->tbase, (const int*)B->tkp, q, nval, ndi, b, x, x64,
+                                      c->d_status, wait_budget_ns(), (unsigned)B->backoff_ns));
     return 0;
 }
 
 int batch_residual(sptrsv_batch_s* B, const double* b, const double* x, cudaStream_t s)
 {
-    if (B->chunked) {
-        k_residual_vkc<<<grid_for((long long)B->n * 32, 256), 256, 0, s>>>(B->nptr, B->ncol, B->nval64, B->ndg64,
-                                                                          B->row_sys, B->sys_row0, B->sys_k,
-                                                                          B->sys_off, B->n, b, x, B->w32b);
-    } else {
-        BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
-        k_residual_vk<<<grid_for((long long)B->ntasks * 32, 256), 256, 0, s>>>(bm, B->val64, B->dg64, B->ntasks,
-                                                                                B->tbase, B->tkp, b, x, B->w32b);
-    }
+    k_residual_nat<<<grid_for((long long)B->nres_tasks * 32, 256), 256, 0, s>>>(
+        B->nptr, B->ncol, B->nval64, B->ndg64, B->sys_task0, B->nsys, B->sys_row0, B->sys_k, B->d_kplog, B->sys_off, b,
+        x, B->w32b);
     SPT_CUDA(cudaGetLastError());
     return 0;
 }
@@ -522,13 +1006,11 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
     // device scratch
     sp_mat_t U{};
     dfr_analysis_info_t info{};
-    int *d_sys = nullptr, *d_row0 = nullptr, *d_kplog = nullptr, *d_sk = nullptr, *key = nullptr, *ord = nullptr;
-    int *kt = nullptr, *vt = nullptr, *scr = nullptr, *pos_of = nullptr;
+    int *d_sys = nullptr, *d_row0 = nullptr, *d_kplog = nullptr, *d_sk = nullptr;
     long long* d_soff = nullptr;
     auto cleanup = [&]() {
         cudaFree(U.ia); cudaFree(U.ja); cudaFree(U.a);
         cudaFree(d_sys); cudaFree(d_row0); cudaFree(d_kplog); cudaFree(d_sk); cudaFree(d_soff);
-        cudaFree(key); cudaFree(ord); cudaFree(kt); cudaFree(vt); cudaFree(scr); cudaFree(pos_of);
     };
     auto fail = [&](int code) {
         cleanup();
@@ -569,7 +1051,7 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
     }
     AnalysisRec* rec = find_analysis(info.row_ctr);
     B->nlevs = info.nlevs;
-    // 3. order (level, rhs class), stable in the natural order
+    // 3. per-system arrays
     BCHK(dalloc(&d_sys, n));
     BCHK(dalloc(&d_row0, nsys + 1));
     BCHK(dalloc(&d_kplog, nsys));
@@ -580,36 +1062,33 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
     BCHK(cudaMemcpy(d_kplog, kplog.data(), sizeof(int) * (size_t)nsys, cudaMemcpyHostToDevice));
     BCHK(cudaMemcpy(d_sk, nrhs, sizeof(int) * (size_t)nsys, cudaMemcpyHostToDevice));
     BCHK(cudaMemcpy(d_soff, B->off.data(), sizeof(long long) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
-    BCHK(dalloc(&key, n));
-    BCHK(dalloc(&ord, n));
-    BCHK(dalloc(&kt, n));
-    BCHK(dalloc(&vt, n));
-    long long sc1 = radix_scratch_ints(n), sc2 = scan_scratch_ints(n + 1);
-    BCHK(dalloc(&scr, sc1 > sc2 ? sc1 : sc2));
-    k_batch_keys<<<grid_for(n, 256), 256, 0, s>>>(rec->d_levels, d_sys, d_kplog, (int)n, key, ord);
-    BCHK(cudaGetLastError());
-    BCHK(radix_sort_pairs(key, ord, kt, vt, n, 6 * info.nlevs - 1, scr, s));
-    // 4. layout
-    BCHK(dalloc(&B->ptr, n + 1));
-    BCHK(dalloc(&pos_of, n));
-    k_batch_rows<<<grid_for(n + 1, 256), 256, 0, s>>>(ord, U.ia, (int)n, B->ptr, pos_of);
-    BCHK(cudaGetLastError());
-    BCHK(scan_exclusive(B->ptr, B->ptr, n + 1, scr, s));
-    BCHK(dalloc(&B->xrow, n));
-    BCHK(dalloc(&B->krow, n));
-    BCHK(dalloc(&B->xdep, B->m));
-    BCHK(dalloc(&B->val64, B->m));
-    BCHK(dalloc(&B->val32, B->m));
-    BCHK(dalloc(&B->dg64, n));
-    BCHK(dalloc(&B->di64, n));
-    BCHK(dalloc(&B->di32, n));
-    k_batch_fill<<<grid_for(n * 32, 256), 256, 0, s>>>(ord, U.ia, U.ja, U.a, d_sys, d_row0, d_soff, d_sk, B->ptr,
-                                                        (int)n, B->xrow, B->krow, B->xdep, B->val64, B->val32,
-                                                        B->dg64, B->di64, B->di32);
-    BCHK(cudaGetLastError());
+    // 4. levels kept per union row; levels of each system
+    BCHK(dalloc(&B->lev, n));
+    BCHK(cudaMemcpyAsync(B->lev, rec->d_levels, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
     {
-        int e = batch_tasks(B, key, 6 * info.nlevs, s);
-        if (e) return fail(e);
+        int* d_nl = nullptr;
+        BCHK(dalloc(&d_nl, nsys));
+        k_sys_nlevs<<<std::min(nsys, 4096), 256, 0, s>>>(B->lev, d_row0, nsys, d_nl);
+        B->sys_nlev.assign(nsys, 0);
+        cudaError_t ce = cudaGetLastError();
+        if (ce == cudaSuccess)
+            ce = cudaMemcpy(B->sys_nlev.data(), d_nl, sizeof(int) * (size_t)nsys, cudaMemcpyDeviceToHost);
+        cudaFree(d_nl);
+        BCHK(ce);
+    }
+    B->row0h = row0;
+    {  // residual tasks: 32/kp consecutive rows of one system each
+        std::vector<int> t0(nsys + 1, 0);
+        long long tot = 0;
+        for (int k = 0; k < nsys; k++) {
+            t0[k] = (int)tot;
+            const int rows = 32 >> kplog[k];
+            tot += (mats[k].nr + rows - 1) / rows;
+        }
+        t0[nsys] = (int)tot;
+        B->nres_tasks = (int)tot;
+        BCHK(dalloc(&B->sys_task0, nsys + 1));
+        BCHK(cudaMemcpy(B->sys_task0, t0.data(), sizeof(int) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
     }
     // 5. natural-order chunk schedule: union without diagonals, chunk tasks in
     //    (chunk index, system) order, each with the first chunk it reads
@@ -668,8 +1147,26 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
         BCHK(cudaMemcpy(B->tj, tjv.data(), sizeof(int) * tjv.size(), cudaMemcpyHostToDevice));
         BCHK(cudaMemcpy(B->cdep, td.data(), sizeof(int) * td.size(), cudaMemcpyHostToDevice));
     }
-    B->row_sys = d_sys;  // kept for the natural-order residual
+    {
+        int* d_md = nullptr;
+        BCHK(dalloc(&d_md, nsys));
+        k_sys_dist<<<std::min(nsys, 4096), 256, 0, s>>>(B->nptr, B->ncol, d_row0, nsys, d_md);
+        B->sys_dist.assign(nsys, 0);
+        cudaError_t ce = cudaGetLastError();
+        if (ce == cudaSuccess)
+            ce = cudaMemcpy(B->sys_dist.data(), d_md, sizeof(int) * (size_t)nsys, cudaMemcpyDeviceToHost);
+        cudaFree(d_md);
+        BCHK(ce);
+    }
+    B->row_sys = d_sys;  // kept for the natural-order residual and the level layout
     d_sys = nullptr;
+    B->d_kplog = d_kplog;
+    d_kplog = nullptr;
+    // 6. sequential systems and the level layout of the others (mode 2)
+    {
+        int e = batch_apply_schedule(B, s);
+        if (e) return fail(e);
+    }
     BCHK(dalloc(&B->w32a, B->nvec));
     BCHK(dalloc(&B->w32b, B->nvec));
     BCHK(cudaStreamSynchronize(s));
@@ -698,15 +1195,15 @@ int sptrsv_batch_info(sptrsv_batch_t B, long long* offsets, int* n_total, int* n
     return ok();
 }
 
-int sptrsv_batch_set_schedule(sptrsv_batch_t B, int chunked, int block_warps, int warps_per_sm, int backoff_ns,
+int sptrsv_batch_set_schedule(sptrsv_batch_t B, int mode, int block_warps, int warps_per_sm, int backoff_ns,
                               int ir_iters)
 {
-    if (!B || (chunked != 0 && chunked != 1) ||
+    if (!B || mode < kModeLevel || mode > kModeHybrid ||
         (block_warps != 2 && block_warps != 4 && block_warps != 8 && block_warps != 16) ||
-        (chunked && block_warps > 8) || warps_per_sm < 0 || warps_per_sm > 64 || backoff_ns < 0 ||
+        (mode == kModeChunk && block_warps > 8) || warps_per_sm < 0 || warps_per_sm > 64 || backoff_ns < 0 ||
         backoff_ns > 100000 || ir_iters < 0 || ir_iters > 16)
         return set_error(SPTRSV_ERR_INVALID_ARG, "batch_set_schedule: bad arguments");
-    B->chunked = chunked;
+    B->mode = mode;
     B->block_warps = block_warps;
     B->warps_per_sm = warps_per_sm;
     B->backoff_ns = backoff_ns;
@@ -715,6 +1212,30 @@ int sptrsv_batch_set_schedule(sptrsv_batch_t B, int chunked, int block_warps, in
         cudaGraphExecDestroy(B->gexec);
         B->gexec = nullptr;
     }
+    int e = batch_apply_schedule(B, 0);
+    return e ? e : ok();
+}
+
+int sptrsv_batch_set_seq_width(sptrsv_batch_t B, double width)
+{
+    if (!B || !(width >= 0.0) || width > 1e9) return set_error(SPTRSV_ERR_INVALID_ARG, "batch_set_seq_width: bad arguments");
+    B->seq_width = width;
+    if (B->gexec) {
+        cudaGraphExecDestroy(B->gexec);
+        B->gexec = nullptr;
+    }
+    int e = batch_apply_schedule(B, 0);
+    return e ? e : ok();
+}
+
+int sptrsv_batch_seq_systems(sptrsv_batch_t B, int* nseq, int* nseq_warps, int* n_level_rows)
+{
+    if (!B) return set_error(SPTRSV_ERR_INVALID_ARG, "batch_seq_systems: NULL");
+    int c = 0;
+    for (char f : B->seq) c += f ? 1 : 0;
+    if (nseq) *nseq = c;
+    if (nseq_warps) *nseq_warps = B->nseqw;
+    if (n_level_rows) *n_level_rows = B->n_lvl;
     return ok();
 }
 

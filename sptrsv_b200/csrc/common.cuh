@@ -190,6 +190,53 @@ __device__ __forceinline__ bool warp_wait(bool pending, int c, const T* x, const
     }
 }
 
+// warp_wait for U values per lane at once: the first nh (per lane) of
+// x[c[0..U)] are loaded back to back, so their latencies overlap, and the warp
+// spins (convergently, with the same budget and abort rules) only while some
+// lane still holds a pending one.  With SMEM, c < 0 reads xs[~c].  Must be
+// called by all 32 lanes; returns false (warp-uniform) on timeout or abort.
+template <bool SMEM, int U, typename T, typename I>
+__device__ __forceinline__ bool warp_wait_n(int nh, const I (&c)[U], const T* x, const volatile T* xs, T (&xv)[U],
+                                            DevStatus* st, unsigned long long budget, unsigned backoff, int row)
+{
+    unsigned pend = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        if (u < nh) {
+            xv[u] = (SMEM && c[u] < 0) ? xs[~c[u]] : ld_relaxed(x + c[u]);
+            if (is_pending(xv[u])) pend |= 1u << u;
+        }
+    }
+    if (!__any_sync(0xffffffffu, pend != 0)) return true;
+    unsigned long long t0 = 0;
+    unsigned it = 0;
+    while (true) {
+        ++it;
+        if (backoff && it > 8) __nanosleep(backoff);
+        if ((it & 63u) == 0) {
+            int stop = 0;
+            if ((threadIdx.x & 31) == 0) {
+                unsigned long long now = global_ns();
+                if (t0 == 0) t0 = now;
+                if (ld_relaxed(&st->code) != 0) stop = 1;
+                else if (now - t0 > budget) {
+                    report(st, SPTRSV_ERR_TIMEOUT, row);
+                    stop = 1;
+                }
+            }
+            if (__shfl_sync(0xffffffffu, stop, 0)) return false;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if ((pend >> u) & 1u) {
+                xv[u] = (SMEM && c[u] < 0) ? xs[~c[u]] : ld_relaxed(x + c[u]);
+                if (!is_pending(xv[u])) pend &= ~(1u << u);
+            }
+        }
+        if (!__any_sync(0xffffffffu, pend != 0)) return true;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T sentinel_value();
 template <>

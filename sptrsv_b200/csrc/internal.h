@@ -41,9 +41,9 @@ int sync_status(cudaStream_t stream);
 // capped by `max_blocks` and by `cap_per_sm` blocks per SM (0: no cap).
 // Launched cooperatively so the co-residency that the static round-robin
 // schedule relies on is guaranteed by the driver.
-template <typename... KArgs, typename... Args>
-cudaError_t launch_persistent_capped(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks,
-                                     int cap_per_sm, cudaStream_t s, Args... args)
+template <typename... KArgs>
+cudaError_t persistent_grid(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks, int cap_per_sm,
+                            long long* grid_out)
 {
     static std::mutex mu;
     static std::unordered_map<long long, int> occ;  // (kernel, block, smem, device) -> blocks per SM
@@ -66,6 +66,20 @@ cudaError_t launch_persistent_capped(void (*kern)(KArgs...), int block, size_t s
     long long grid = (long long)per_sm * c->num_sms;
     if (max_blocks < grid) grid = max_blocks;
     if (grid < 1) grid = 1;
+    *grid_out = grid;
+    return cudaSuccess;
+}
+
+// Cooperative launch of a persistent kernel: blocks per SM from the
+// occupancy calculator (optionally capped), at most max_blocks blocks, all
+// co-resident.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_persistent_capped(void (*kern)(KArgs...), int block, size_t smem, long long max_blocks,
+                                     int cap_per_sm, cudaStream_t s, Args... args)
+{
+    long long grid = 0;
+    cudaError_t e = persistent_grid(kern, block, smem, max_blocks, cap_per_sm, &grid);
+    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3((unsigned)block);

@@ -33,6 +33,23 @@ struct SptLayout {
     float* di32 = nullptr;   // 1.0f / (float)diagonal
 };
 
+// STRIP schedule (built on demand, see strip.cu).  Arrays are in processing
+// order: slot P * 32 + j is row j of the chunk at position P (strips
+// contiguous, positions of a strip in its wavefront order).
+struct StripLayout {
+    int* row = nullptr;        // [npos*32] natural row of the slot, -1 past the last row
+    int* pe = nullptr;         // [npos*32+1] first entry of the slot (entries before its chunk)
+    int* ecol = nullptr;       // column, or ~ring slot for a chunk this warp solved recently
+    double* ev64 = nullptr;
+    float* ev32 = nullptr;
+    double* lsub64 = nullptr;  // [npos*32] L(i, i-1) when row i-1 is in the same chunk, else 0
+    float* lsub32 = nullptr;
+    double* di64 = nullptr;    // [npos*32] 1 / diagonal
+    float* di32 = nullptr;
+    int* sptr = nullptr;       // [nstrips+1] first position of each strip
+    int nstrips = 0, R = 0, W = 0;
+};
+
 struct sptrsv_plan_s {
     int device = -1;
     int n = 0, nnz_off = 0, nlevs = 0, n_warps = 0;
@@ -50,6 +67,8 @@ struct sptrsv_plan_s {
     int* clu_tasks = nullptr;    // (cluster, level)-aligned tasks
     int* clu_ctask = nullptr;    // first task of each cluster [nclusters+1]
     int clu_ntasks = 0, clu_R = 0;
+    StripLayout strip;           // STRIP layout (built on demand)
+    int row_strip_R = 0;         // R the strip layout was built for (0: none)
     float* w32a = nullptr;
     float* w32b = nullptr;
     int cap_rhs = 0;
@@ -67,4 +86,8 @@ int build_cluster_layout(sptrsv_plan_s* p, int H, int B);
 // Level-aligned task tables with R rows per task (cached per R).
 int build_order_tasks(sptrsv_plan_s* p, int R);
 int build_cluster_tasks(sptrsv_plan_s* p, int R);
+// Builds (or keeps) p->strip for R runs per strip; SPTRSV_ERR_UNSUPPORTED
+// when the matrix does not have the chunk structure.
+int build_strip_layout(sptrsv_plan_s* p, int R);
+void strip_free(StripLayout& t);
 }  // namespace sptrsv

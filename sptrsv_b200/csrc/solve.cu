@@ -16,6 +16,12 @@ constexpr int kRefWarps = kRefBlock / 32;
 
 bool pow2_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32; }
 
+// Shared memory of the STRIP kernel: per warp a ring of 2R chunks of 32 values.
+size_t strip_smem_bytes(const sptrsv_schedule_t* s, size_t elem)
+{
+    return (size_t)s->block_warps * 2 * s->rows_per_warp * 32 * elem;
+}
+
 __global__ void k_iorder_level_keys(const int* __restrict__ iorder, const int* __restrict__ level, int n,
                                     int* __restrict__ key)
 {
@@ -149,6 +155,7 @@ void plan_free_arrays(sptrsv_plan_s* p)
 {
     layout_free(p->lev);
     layout_free(p->clu);
+    strip_free(p->strip);
     cudaFree(p->cptr); cudaFree(p->inv); cudaFree(p->levels); cudaFree(p->ibase); cudaFree(p->ivect);
     for (int j = 0; j < 6; j++) cudaFree(p->ord_tasks[j]);
     cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
@@ -189,6 +196,14 @@ int plan_fill_values(sptrsv_plan_s* p, const sp_mat_t* L, cudaStream_t s)
         p->clu_H = 0;
         SPT_CUDA(cudaStreamSynchronize(s));
         int e = build_cluster_layout(p, H, B);
+        if (e) return e;
+    }
+    if (p->strip.row) {  // and the strip copy
+        const int R = p->strip.R;
+        SPT_CUDA(cudaStreamSynchronize(s));
+        strip_free(p->strip);
+        p->row_strip_R = 0;
+        int e = build_strip_layout(p, R);
         if (e) return e;
     }
     return 0;
@@ -242,6 +257,21 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         SPT_CUDA(launch_persistent_capped(kern, block, smem, p->nclusters, cap, s, m, (const int*)p->cptr,
                                           (const int*)p->clu_ctask, (const int*)p->clu_tasks, p->nclusters,
                                           32 / sc.rows_per_warp, b, x, x64, c->d_status, budget, backoff));
+        return 0;
+    }
+    if (sc.variant == SPTRSV_VAR_STRIP && nrhs == 1) {
+        int e = build_strip_layout(p, sc.rows_per_warp);
+        if (e) return e;
+        const StripLayout& t = p->strip;
+        StripMat<V> m{t.row, t.pe, t.ecol,
+                      f32 ? reinterpret_cast<const V*>(t.ev32) : reinterpret_cast<const V*>(t.ev64),
+                      f32 ? reinterpret_cast<const V*>(t.lsub32) : reinterpret_cast<const V*>(t.lsub64),
+                      f32 ? reinterpret_cast<const V*>(t.di32) : reinterpret_cast<const V*>(t.di64), t.sptr};
+        auto kern = k_sptrsv_strip<V, T, BT, OUT>;
+        const size_t smem = (size_t)sc.block_warps * t.W * 32 * sizeof(T);
+        SPT_CUDA(allow_smem(kern, smem));
+        SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(t.nstrips, sc.block_warps), cap, s, m,
+                                          t.nstrips, t.W, b, x, x64, c->d_status, budget, backoff));
         return 0;
     }
     const V *val, *dg, *di;
@@ -427,6 +457,8 @@ int check_schedule(const sptrsv_schedule_t* s)
     if (s->band_levels < 1 || s->band_levels > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: band_levels");
     if (s->cluster_rows < 32 || s->cluster_rows > 8192)
         return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: cluster_rows must be in [32, 8192]");
+    if (s->variant == SPTRSV_VAR_STRIP && strip_smem_bytes(s, 8) > 200 * 1024)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: strip ring does not fit shared memory");
     return 0;
 }
 
@@ -538,6 +570,9 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
         if (e) return e;
     } else if (s->variant == SPTRSV_VAR_ORDER) {
         e = build_order_tasks(p, s->rows_per_warp);
+        if (e) return e;
+    } else if (s->variant == SPTRSV_VAR_STRIP) {
+        e = build_strip_layout(p, s->rows_per_warp);
         if (e) return e;
     }
     p->sched = *s;

@@ -277,9 +277,12 @@ __global__ void __launch_bounds__(512) k_sptrsv_cluster(PermMat<V> m, const int*
 // nrhs right-hand sides (row-major n x K).  kp = power of two >= K lanes per
 // row; level-aligned task t covers positions [tbase[t], tbase[t+1]) (at
 // most 32/kp rows); lane k of a row owns right-hand side k and walks all of
-// the row's elements, the warp waiting for each round together.
+// the row's elements, kMrhsU per round: their columns, then their x values,
+// are loaded back to back and the warp waits for the round together.  The
+// products are subtracted in element order.
+constexpr int kMrhsU = 8;
 template <class M, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(512) k_sptrsv_mrhs(M m, int ntasks, const int* __restrict__ tbase, int K, int kp,
+__global__ void __launch_bounds__(512, 1) k_sptrsv_mrhs(M m, int ntasks, const int* __restrict__ tbase, int K, int kp,
                                                      const BT* __restrict__ b, T* x, double* x64, DevStatus* st,
                                                      unsigned long long budget, unsigned backoff)
 {
@@ -300,20 +303,160 @@ __global__ void __launch_bounds__(512) k_sptrsv_mrhs(M m, int ntasks, const int*
             len = q.e - q.s;
         }
         const int rounds = __reduce_max_sync(0xffffffffu, len);
-        for (int j = 0; j < rounds; j++) {
-            const bool have = j < len;
-            int c = 0;
-            T v = 0, xv = 0;
-            if (have) {
-                c = m.c(q.s + j);
-                v = (T)m.v(q.s + j);
+        for (int j = 0; j < rounds; j += kMrhsU) {
+            const int nh = min(kMrhsU, len - j);
+            long long ci[kMrhsU];
+            T vv[kMrhsU], xv[kMrhsU];
+#pragma unroll
+            for (int u = 0; u < kMrhsU; u++) {
+                ci[u] = 0;
+                vv[u] = 0;
+                if (u < nh) {
+                    ci[u] = (long long)m.c(q.s + j + u) * K + k;
+                    vv[u] = (T)m.v(q.s + j + u);
+                }
             }
-            if (!warp_wait<false, T>(have, (int)((size_t)c * K + k), x, nullptr, xv, st, budget, backoff,
-                                     act ? q.r : -1))
-                return;
-            if (have) acc -= v * xv;
+            if (!warp_wait_n<false, kMrhsU, T>(nh, ci, x, nullptr, xv, st, budget, backoff, act ? q.r : -1)) return;
+#pragma unroll
+            for (int u = 0; u < kMrhsU; u++)
+                if (u < nh) acc -= vv[u] * xv[u];
         }
         if (act) publish<T, OUT>(x, x64, (size_t)q.r * K + k, acc * piv);
+    }
+}
+
+// STRIP schedule (see strip.cu): warp w takes strips w, w + nw, ...; in a
+// strip it solves chunk after chunk in wavefront order.  Lane j owns row j
+// of the chunk at position P (slot P * 32 + j of the processing-order
+// layout): it subtracts the row's entries outside the chunk (ring slots ~c
+// from shared memory, other columns from x with the warp-convergent wait,
+// kStripU per round), then the warp evaluates x_j = alpha_j + beta_j x_{j-1}
+// by an affine Kogge-Stone scan: after the step of distance d lane j holds
+// the composition of the maps j-2d+1..j, (alpha, beta) <- (alpha + beta *
+// alpha', beta * beta') with (alpha', beta') from lane j - d; beta of the
+// chunk's first row is 0, so the result is x_j.  A chunk's slot metadata is
+// loaded two positions ahead and its entries and right-hand side one
+// position ahead, so no load of the next chunk waits on another load.
+template <typename V>
+struct StripMat {
+    const int* __restrict__ row;
+    const int* __restrict__ pe;
+    const int* __restrict__ ecol;
+    const V* __restrict__ ev;
+    const V* __restrict__ lsub;
+    const V* __restrict__ di;
+    const int* __restrict__ sptr;
+};
+
+constexpr int kStripU = 4;
+
+template <typename T>
+struct StripMeta {
+    int row, e0, e1;
+    T piv, lsub;
+};
+
+template <typename T>
+struct StripEnt {
+    T b;
+    int cc[kStripU];
+    T vv[kStripU];
+};
+
+template <typename V, typename T>
+__device__ __forceinline__ void strip_meta(StripMeta<T>& z, const StripMat<V>& m, int slot)
+{
+    z.row = __ldg(m.row + slot);
+    z.e0 = __ldg(m.pe + slot);
+    z.e1 = __ldg(m.pe + slot + 1);
+    z.piv = (T)__ldg(m.di + slot);
+    z.lsub = (T)__ldg(m.lsub + slot);
+}
+
+template <typename V, typename T, typename BT>
+__device__ __forceinline__ void strip_ent(StripEnt<T>& z, const StripMeta<T>& md, const StripMat<V>& m,
+                                          const BT* __restrict__ b)
+{
+    z.b = md.row >= 0 ? (T)b[md.row] : (T)0;
+#pragma unroll
+    for (int u = 0; u < kStripU; u++) {
+        z.cc[u] = 0;
+        z.vv[u] = 0;
+        if (md.e0 + u < md.e1) {
+            z.cc[u] = __ldg(m.ecol + md.e0 + u);
+            z.vv[u] = (T)__ldg(m.ev + md.e0 + u);
+        }
+    }
+}
+
+template <typename V, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstrips, int W, const BT* __restrict__ b,
+                                                      T* x, double* x64, DevStatus* st, unsigned long long budget,
+                                                      unsigned backoff)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T* ring = reinterpret_cast<T*>(smem_raw) + (size_t)wib * W * 32;
+    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    for (int sidx = gw; sidx < nstrips; sidx += nw) {
+        const int P0 = __ldg(m.sptr + sidx), P1 = __ldg(m.sptr + sidx + 1);
+        StripMeta<T> m0, m1;
+        StripEnt<T> e0;
+        strip_meta<V, T>(m0, m, P0 * 32 + lane);
+        strip_ent<V, T, BT>(e0, m0, m, b);
+        if (P0 + 1 < P1) strip_meta<V, T>(m1, m, (P0 + 1) * 32 + lane);
+        for (int P = P0; P < P1; P++) {
+            const StripMeta<T> md = m0;
+            const StripEnt<T> en = e0;
+            if (P + 1 < P1) {
+                m0 = m1;
+                strip_ent<V, T, BT>(e0, m0, m, b);
+                if (P + 2 < P1) strip_meta<V, T>(m1, m, (P + 2) * 32 + lane);
+            }
+            const int pos = P - P0;
+            const int ec = md.e1 - md.e0;
+            T acc = en.b;
+            const int rounds = __reduce_max_sync(FULL, ec);
+            for (int j = 0; j < rounds; j += kStripU) {
+                const int nh = min(kStripU, ec - j);
+                int cc[kStripU];
+                T vv[kStripU], xv[kStripU];
+#pragma unroll
+                for (int u = 0; u < kStripU; u++) {
+                    cc[u] = en.cc[u];
+                    vv[u] = en.vv[u];
+                    if (j > 0) {
+                        cc[u] = 0;
+                        vv[u] = 0;
+                        if (u < nh) {
+                            cc[u] = __ldg(m.ecol + md.e0 + j + u);
+                            vv[u] = (T)__ldg(m.ev + md.e0 + j + u);
+                        }
+                    }
+                }
+                if (!warp_wait_n<true, kStripU, T>(nh, cc, x, ring, xv, st, budget, backoff, md.row)) return;
+#pragma unroll
+                for (int u = 0; u < kStripU; u++)
+                    if (u < nh) acc -= vv[u] * xv[u];
+            }
+            T a = acc * md.piv, bb = -md.lsub * md.piv;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T ap = __shfl_up_sync(FULL, a, d), bp = __shfl_up_sync(FULL, bb, d);
+                if (lane >= d) {
+                    a = a + bb * ap;
+                    bb = bb * bp;
+                }
+            }
+            const T xi = publishable(a);
+            if (md.row >= 0) {
+                ring[(pos % W) * 32 + lane] = xi;
+                publish<T, OUT>(x, x64, md.row, xi);
+            }
+            __syncwarp();
+        }
     }
 }
 

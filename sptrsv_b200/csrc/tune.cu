@@ -1,12 +1,14 @@
 // tune.cu — the schedule classes, the exhaustive autotuner and the MLP's
 // schedule prediction.
 //
-// 24 classes = 4 variants x 6 parameter presets.  For SIMPLE and ORDER the
-// preset is rows per warp (1..32, i.e. 32..1 lanes per row — the reference's
-// six tile sizes, analysis_csr.cu:84-102).  MULTIROW takes lanes per row from
-// the analysis map, so its presets vary the polling back-off and the number
-// of resident warps.  CLUSTER presets vary band height, cluster size and
-// lanes per row.
+// 24 classes = 4 groups x 6 parameter presets.  The natural-order group holds
+// SIMPLE with 1 and 32 rows per task and STRIP with 1, 2, 8 and 16 grid lines
+// per warp (STRIP applies only to matrices with its chunk structure; elsewhere
+// its classes fail to set and are skipped).  For ORDER the preset is rows per
+// warp (1..32, i.e. 32..1 lanes per row — the reference's six tile sizes,
+// analysis_csr.cu:84-102).  MULTIROW takes lanes per row from the analysis
+// map, so its presets vary the polling back-off and the number of resident
+// warps.  CLUSTER presets vary band height, cluster size and lanes per row.
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -28,11 +30,17 @@ int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
 {
     if (!s || cls < 0 || cls >= SPTRSV_N_CLASSES) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule_from_class: bad class");
     static const int rpw[6] = {1, 2, 4, 8, 16, 32};
+    // natural-order group: SIMPLE with 1 and 32 rows per task; STRIP with
+    // 1, 2, 8, 16 grid lines per warp in between
+    static const int strip_r[6] = {0, 1, 2, 8, 16, 0};
+    static const int strip_bw[6] = {0, 2, 4, 4, 8, 0};
     // MULTIROW presets: block warps, back-off ns, resident warps per SM
     static const int mr[6][3] = {{8, 0, 0}, {8, 200, 0}, {8, 1000, 0}, {4, 0, 16}, {8, 200, 32}, {16, 0, 0}};
     // CLUSTER presets: band levels, cluster rows, rows per warp, block warps
-    static const int cl[6][4] = {{16, 1024, 16, 4}, {32, 2048, 16, 8}, {64, 4096, 16, 8},
-                                 {64, 4096, 32, 8}, {128, 8192, 16, 16}, {128, 8192, 32, 16}};
+    // (from sweeps of H = 16..4096, B = 1024..8192 on banded and grid matrices:
+    // wide bands with 16 rows per task and 16-warp blocks lead)
+    static const int cl[6][4] = {{64, 4096, 16, 8},    {128, 4096, 16, 16}, {256, 2048, 16, 16},
+                                 {256, 4096, 16, 16},  {512, 8192, 16, 16}, {4096, 2048, 16, 8}};
     const int v = cls / 6, j = cls % 6;
     s->variant = v;
     s->rows_per_warp = 1;
@@ -42,7 +50,11 @@ int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
     s->ir_max_iters = 2;
     s->band_levels = 64;
     s->cluster_rows = 4096;
-    if (v == SPTRSV_VAR_SIMPLE || v == SPTRSV_VAR_ORDER) {
+    if (v == SPTRSV_VAR_SIMPLE && strip_r[j]) {
+        s->variant = SPTRSV_VAR_STRIP;
+        s->rows_per_warp = strip_r[j];
+        s->block_warps = strip_bw[j];
+    } else if (v == SPTRSV_VAR_SIMPLE || v == SPTRSV_VAR_ORDER) {
         s->rows_per_warp = rpw[j];
     } else if (v == SPTRSV_VAR_MULTIROW) {
         s->block_warps = mr[j][0];
@@ -141,16 +153,24 @@ int sptrsv_plan_select_schedule(sptrsv_plan_t p, sptrsv_mlp_t M, const sp_mat_t*
     float f[12];
     int e = sptrsv_features(L, info, f);
     if (e) return e;
-    int cls = 0;
-    e = sptrsv_mlp_predict_class(M, f, &cls);
+    // classes in order of predicted time; the first one that applies to
+    // this matrix (a STRIP class needs its chunk structure) is set
+    float out[SPTRSV_N_CLASSES];
+    e = sptrsv_mlp_forward_host(M, f, 1, out);
     if (e) return e;
-    sptrsv_schedule_t s;
-    sptrsv_schedule_from_class(cls, &s);
-    s.ir_max_iters = p->sched.ir_max_iters;
-    e = sptrsv_plan_set_schedule(p, &s);
-    if (e) return e;
-    if (cls_out) *cls_out = cls;
-    return ok();
+    int order[SPTRSV_N_CLASSES];
+    for (int k = 0; k < SPTRSV_N_CLASSES; k++) order[k] = k;
+    std::stable_sort(order, order + SPTRSV_N_CLASSES, [&](int a, int b) { return out[a] < out[b]; });
+    for (int k = 0; k < SPTRSV_N_CLASSES; k++) {
+        sptrsv_schedule_t s;
+        sptrsv_schedule_from_class(order[k], &s);
+        s.ir_max_iters = p->sched.ir_max_iters;
+        if (sptrsv_plan_set_schedule(p, &s) == 0) {
+            if (cls_out) *cls_out = order[k];
+            return ok();
+        }
+    }
+    return set_error(SPTRSV_ERR_UNSUPPORTED, "select_schedule: no class applies");
 }
 
 }  // extern "C"

@@ -31,15 +31,24 @@ def test_batch_matches_oracle_per_system(torch_cuda, precision):
     assert np.array_equal(np.diff(batch.offsets), [m.n * k for m, k in zip(mats, ks)])
     db = torch.from_numpy(np.concatenate(bs)).cuda()
     dx = torch.empty_like(db)
-    for sched in (dict(), dict(chunked=1, block_warps=4, warps_per_sm=16), dict(chunked=0),
-                  dict(chunked=0, block_warps=4, warps_per_sm=16), dict(chunked=0, block_warps=16, backoff_ns=100)):
+    for sched, width in ((dict(), None), (dict(mode=1, block_warps=4, warps_per_sm=16), None), (dict(mode=0), None),
+                         (dict(mode=0, block_warps=4, warps_per_sm=16), None),
+                         (dict(mode=0, block_warps=16, backoff_ns=100), None),
+                         (dict(mode=2), 16.0), (dict(mode=2, block_warps=4), 1e9), (dict(mode=2, block_warps=2), 4.0),
+                         (dict(mode=2, block_warps=16), 0.0)):
+        if width is not None:
+            batch.set_seq_width(width)
         batch.set_schedule(**sched)
+        if width == 1e9:
+            assert batch.seq_systems()[0] == len(mats) and batch.seq_systems()[2] == 0
+        if width == 0.0:
+            assert batch.seq_systems() == (0, 0, batch.n)
         batch.solve(db, dx, precision)
         S.sync_status()
         xh = dx.cpu().numpy()
         for s in range(len(mats)):
             a, b = batch.offsets[s], batch.offsets[s + 1]
-            assert O.rel_err(xh[a:b], refs[s]) <= TOL, (s, sched)
+            assert O.rel_err(xh[a:b], refs[s]) <= TOL, (s, sched, width)
     batch.close()
     for d in dev:
         S.free_device_analysis(d, None)
@@ -88,10 +97,44 @@ def test_batch_unit_values_exact(torch_cuda):
     b = np.concatenate([np.repeat(np.diff(m.rowptr).astype(np.float64), k) for m, k in zip(units, ks)])
     db = torch.from_numpy(b).cuda()
     dx = torch.empty_like(db)
-    for prec in (64, 32):
-        batch.solve(db, dx, prec)
+    batch.set_seq_width(1e9)
+    for mode in (0, 1, 2):
+        batch.set_schedule(mode=mode, block_warps=4)
+        for prec in (64, 32):
+            batch.solve(db, dx, prec)
+            S.sync_status()
+            assert bool((dx == 1.0).all()), (mode, prec)
+    batch.close()
+    for d in dev:
+        S.free_device_analysis(d, None)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_hybrid_many_systems_per_warp(torch_cuda, precision):
+    """More near-chain systems than sequential warps: each warp walks several
+    systems one after another (one block of two warps per SM)."""
+    import sptrsv_b200 as S
+    from sptrsv_b200.batch import Batch
+
+    torch = torch_cuda
+    mats, ks, xs = gen.batch_config(400, seed=11, n_lo=40, n_hi=300, bw_lo=2, bw_hi=40)
+    dev = [S.allocate_memory(m.rowptr, m.colidx, m.val, m.n) for m in mats]
+    bs = [m.matvec(x, k) for m, x, k in zip(mats, xs, ks)]
+    refs = [O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k) for m, b, k in zip(mats, bs, ks)]
+    batch = Batch(dev, ks)
+    batch.set_seq_width(1e9)
+    batch.set_schedule(mode=2, block_warps=2, warps_per_sm=2)
+    nseq, nw, nlvl = batch.seq_systems()
+    assert nseq == len(mats) and nlvl == 0 and 0 < nw < nseq
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.empty_like(db)
+    for rep in range(2):
+        batch.solve_graph(db, dx, precision)
         S.sync_status()
-        assert bool((dx == 1.0).all()), prec
+        xh = dx.cpu().numpy()
+        for s in range(len(mats)):
+            a, b = batch.offsets[s], batch.offsets[s + 1]
+            assert O.rel_err(xh[a:b], refs[s]) <= TOL, (rep, s)
     batch.close()
     for d in dev:
         S.free_device_analysis(d, None)

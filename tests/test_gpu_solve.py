@@ -266,3 +266,105 @@ def test_solves_match_reference_golden(torch_cuda, path):
     assert O.rel_err(x, g["ref_x_multirow"]) <= TOL
     plan.close()
     S.free_device_analysis(L, info)
+
+
+STRIP_OK = {
+    "grid2d_aligned": lambda: gen.grid2d(160, 140, seed=1),
+    "grid2d_ragged": lambda: gen.grid2d(100, 77, seed=2),
+    "grid3d": lambda: gen.grid3d(40, 20, 15, seed=3),
+    "grid3d_ragged": lambda: gen.grid3d(45, 13, 9, seed=4),
+    "grid2d_short_lines": lambda: gen.grid2d(20, 90, seed=5),
+}
+
+
+@pytest.mark.parametrize("name", list(STRIP_OK))
+def test_strip_schedule_fp64_and_ir(torch_cuda, name):
+    """The STRIP schedule (prefix scan over 32-row chunks, grid lines per warp
+    in wavefront order) against the oracle, for several lines per warp."""
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = STRIP_OK[name]()
+    xt = gen.vector(m.n, "uniform", seed=9)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
+    for r, bw in ((1, 4), (2, 2), (4, 4), (8, 4), (16, 4), (32, 2)):
+        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=bw, ir_max_iters=2)
+        for rep in range(2):
+            plan.solve_f64(db, dx)
+            S.sync_status()
+            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, (r, bw, rep)
+        plan.solve_ir(db, dx)
+        S.sync_status()
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", r, bw)
+    # new values, same pattern: the strip copy is rebuilt
+    m2 = gen.HostCsr(m.rowptr, m.colidx, m.val * 1.5)
+    L2 = S.allocate_memory(m2.rowptr, m2.colidx, m2.val, m2.n)
+    plan.update_values(L2)
+    plan.solve_f64(db, dx)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref / 1.5) <= TOL
+    plan.close()
+    S.free_device_analysis(L2, None)
+    S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("name", ["banded", "zipf"])
+def test_strip_schedule_rejects_other_structures(torch_cuda, name):
+    import sptrsv_b200 as S
+
+    m = gen.banded(5000, 64, 4, 8, seed=1) if name == "banded" else gen.zipf(5000, 1.5, 64, seed=1)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    with pytest.raises(S.SptrsvError) as ei:
+        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=4, block_warps=4)
+    assert ei.value.code == S._lib.SPTRSV_ERR_UNSUPPORTED
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+def test_selector_skips_classes_that_do_not_apply(torch_cuda):
+    """A network that ranks a STRIP class first: on a grid it is taken, on a
+    banded matrix the next class in predicted order is."""
+    import sptrsv_b200 as S
+    from sptrsv_b200 import select as SEL
+
+    net = SEL.Mlp(seed=1)
+    p = np.zeros(SEL.N_PARAMS, np.float32)
+    b3 = np.arange(SEL.N_CLASSES, dtype=np.float32)
+    b3[2] = -10.0  # a STRIP class first, then class 0, 1, 3, ...
+    p[-SEL.N_CLASSES:] = b3
+    net.set_params(p)
+    net.set_normalization(np.zeros(SEL.N_FEATURES, np.float32), np.ones(SEL.N_FEATURES, np.float32))
+    for m, want in ((gen.grid2d(96, 64, seed=1), 2), (gen.banded(4000, 64, 4, 8, seed=1), 0)):
+        L, info = _setup(S, m, S.MULTIROW)
+        plan = S.Plan(L, info)
+        assert net.select(plan, L, info) == want
+        assert plan.schedule().variant == SEL.schedule_from_class(want).variant
+        plan.close()
+        S.free_device_analysis(L, info)
+    net.close()
+
+
+def test_strip_full_size_grid(torch_cuda):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m, xt, k = gen.config("c1")
+    b = m.matvec(xt, k)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
+    for r in (4, 8, 16, 32):
+        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=2 if r == 32 else 4)
+        plan.solve_f64(db, dx)
+        S.sync_status()
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, r
+    plan.close()
+    S.free_device_analysis(L, info)

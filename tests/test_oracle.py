@@ -77,6 +77,24 @@ def test_fp64_oracle_against_long_double(name):
     assert O.rel_err(x, xt) <= 1e-12
 
 
+@pytest.mark.parametrize("name", list(_matrices()))
+def test_fp32_restatement(name):
+    """The float restatement of the reference's FP32 build: exact on the
+    reference's known-answer test, within FP32 accuracy of the FP64 oracle,
+    and really computed in float (not the FP64 result rounded)."""
+    m = _matrices()[name]
+    u = m.unit_values()
+    bu = np.diff(u.rowptr).astype(np.float64)
+    assert np.all(O.solve(u.rowptr, u.colidx, u.val, bu, f32=True) == 1.0)
+    xt = gen.vector(m.n, "uniform", seed=3)
+    b = m.matvec(xt)
+    x64 = O.solve(m.rowptr, m.colidx, m.val, b)
+    x32 = O.solve(m.rowptr, m.colidx, m.val, b, f32=True)
+    assert O.rel_err(x32, x64) <= 1e-4
+    assert np.array_equal(x32, x32.astype(np.float32).astype(np.float64))
+    assert not np.array_equal(x32, x64.astype(np.float32).astype(np.float64)) or m.n < 64
+
+
 def test_multi_rhs_oracle_matches_single():
     m = _matrices()["zipf"]
     k = 5
