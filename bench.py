@@ -398,7 +398,7 @@ def run_ours(args, rank, world, local, dist):
 
     if args.lean:
         # profiling run: one fixed schedule, warm-up and the timed steps, nothing else
-        cls = args.fixed_class if args.fixed_class >= 0 else 21  # cluster/H256-B4096-rpw16-bw16
+        cls = args.fixed_class if args.fixed_class >= 0 else 3  # wave/G8
         s = SEL.schedule_from_class(cls)
         s.ir_max_iters = 1
         plan.set_schedule_struct(s)

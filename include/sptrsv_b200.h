@@ -207,7 +207,10 @@ typedef struct sptrsv_plan_s* sptrsv_plan_t;
                                 /* are all on the previous row, solved by a prefix   */
                                 /* scan; rows_per_warp grid lines per warp (1..32),  */
                                 /* wavefront order; SPTRSV_ERR_UNSUPPORTED otherwise */
-#define SPTRSV_N_VARIANTS    5
+#define SPTRSV_VAR_WAVE      5  /* STRIP's chunks; block_warps grid lines per CTA,   */
+                                /* one warp per line, the lines' x in shared memory  */
+                                /* (their rows must fit: 25,600 rows in FP64)        */
+#define SPTRSV_N_VARIANTS    6
 
 typedef struct {
     int variant;          /* SPTRSV_VAR_*                                            */

@@ -27,8 +27,8 @@ SPTRSV_ERR_ALLOC = -7
 SPTRSV_ERR_NOT_CONVERGED = -8
 SPTRSV_ERR_UNSUPPORTED = -9
 
-VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER, VAR_STRIP = 0, 1, 2, 3, 4
-N_VARIANTS = 5
+VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER, VAR_STRIP, VAR_WAVE = 0, 1, 2, 3, 4, 5
+N_VARIANTS = 6
 
 
 class SpMat(ctypes.Structure):

@@ -50,6 +50,26 @@ struct StripLayout {
     int nstrips = 0, R = 0, W = 0;
 };
 
+// WAVE schedule (built on demand, see strip.cu): the strip chunks in natural
+// order (slot = chunk * 32 + lane); G consecutive runs (grid lines) form a
+// group solved by one CTA, one warp per line, with the group's x values in
+// shared memory.
+struct WaveLayout {
+    int* row = nullptr;        // [nch*32] natural row of the slot, -1 past the chunk's last row
+    int* pe = nullptr;         // [nch*32+1] first entry of the slot
+    int* ecol = nullptr;       // column, or ~(column - first row of the group) inside the group
+    double* ev64 = nullptr;
+    float* ev32 = nullptr;
+    double* lsub64 = nullptr;
+    float* lsub32 = nullptr;
+    double* di64 = nullptr;
+    float* di32 = nullptr;
+    int* runc = nullptr;       // [nruns+1] first chunk of each run
+    int* grun = nullptr;       // [ngroups+1] first run of each group
+    int* grow = nullptr;       // [ngroups+1] first row of each group
+    int ngroups = 0, G = 0, cap = 0;  // cap: most rows in one group
+};
+
 struct sptrsv_plan_s {
     int device = -1;
     int n = 0, nnz_off = 0, nlevs = 0, n_warps = 0;
@@ -69,6 +89,7 @@ struct sptrsv_plan_s {
     int clu_ntasks = 0, clu_R = 0;
     StripLayout strip;           // STRIP layout (built on demand)
     int row_strip_R = 0;         // R the strip layout was built for (0: none)
+    WaveLayout wave;             // WAVE layout (built on demand)
     float* w32a = nullptr;
     float* w32b = nullptr;
     int cap_rhs = 0;
@@ -90,4 +111,9 @@ int build_cluster_tasks(sptrsv_plan_s* p, int R);
 // when the matrix does not have the chunk structure.
 int build_strip_layout(sptrsv_plan_s* p, int R);
 void strip_free(StripLayout& t);
+// Builds (or keeps) p->wave for G lines per CTA; SPTRSV_ERR_UNSUPPORTED when
+// the matrix does not have the chunk structure or a group's rows do not fit
+// max_rows.
+int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows);
+void wave_free(WaveLayout& w);
 }  // namespace sptrsv

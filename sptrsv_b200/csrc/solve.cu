@@ -16,6 +16,9 @@ constexpr int kRefWarps = kRefBlock / 32;
 
 bool pow2_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32; }
 
+// Rows of one WAVE line group: their FP64 x values fill the CTA's shared memory.
+constexpr int kWaveMaxRows = 200 * 1024 / 8;
+
 // Shared memory of the STRIP kernel: per warp a ring of 2R chunks of 32 values.
 size_t strip_smem_bytes(const sptrsv_schedule_t* s, size_t elem)
 {
@@ -156,6 +159,7 @@ void plan_free_arrays(sptrsv_plan_s* p)
     layout_free(p->lev);
     layout_free(p->clu);
     strip_free(p->strip);
+    wave_free(p->wave);
     cudaFree(p->cptr); cudaFree(p->inv); cudaFree(p->levels); cudaFree(p->ibase); cudaFree(p->ivect);
     for (int j = 0; j < 6; j++) cudaFree(p->ord_tasks[j]);
     cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
@@ -196,6 +200,13 @@ int plan_fill_values(sptrsv_plan_s* p, const sp_mat_t* L, cudaStream_t s)
         p->clu_H = 0;
         SPT_CUDA(cudaStreamSynchronize(s));
         int e = build_cluster_layout(p, H, B);
+        if (e) return e;
+    }
+    if (p->wave.row) {  // the wave copy
+        const int G = p->wave.G;
+        SPT_CUDA(cudaStreamSynchronize(s));
+        wave_free(p->wave);
+        int e = build_wave_layout(p, G, kWaveMaxRows);
         if (e) return e;
     }
     if (p->strip.row) {  // and the strip copy
@@ -272,6 +283,22 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         SPT_CUDA(allow_smem(kern, smem));
         SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(t.nstrips, sc.block_warps), cap, s, m,
                                           t.nstrips, t.W, b, x, x64, c->d_status, budget, backoff));
+        return 0;
+    }
+    if (sc.variant == SPTRSV_VAR_WAVE && nrhs == 1) {
+        int e = build_wave_layout(p, sc.block_warps, kWaveMaxRows);
+        if (e) return e;
+        const WaveLayout& t = p->wave;
+        WaveMat<V> m{{t.row, t.pe, t.ecol,
+                      f32 ? reinterpret_cast<const V*>(t.ev32) : reinterpret_cast<const V*>(t.ev64),
+                      f32 ? reinterpret_cast<const V*>(t.lsub32) : reinterpret_cast<const V*>(t.lsub64),
+                      f32 ? reinterpret_cast<const V*>(t.di32) : reinterpret_cast<const V*>(t.di64), nullptr},
+                     t.runc, t.grun, t.grow};
+        auto kern = k_sptrsv_wave<V, T, BT, OUT>;
+        const size_t smem = (size_t)t.cap * sizeof(T);
+        SPT_CUDA(allow_smem(kern, smem));
+        SPT_CUDA(launch_persistent_capped(kern, block, smem, t.ngroups, cap, s, m, t.ngroups, b, x, x64, c->d_status,
+                                          budget, backoff));
         return 0;
     }
     const V *val, *dg, *di;
@@ -573,6 +600,9 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
         if (e) return e;
     } else if (s->variant == SPTRSV_VAR_STRIP) {
         e = build_strip_layout(p, s->rows_per_warp);
+        if (e) return e;
+    } else if (s->variant == SPTRSV_VAR_WAVE) {
+        e = build_wave_layout(p, s->block_warps, kWaveMaxRows);
         if (e) return e;
     }
     p->sched = *s;

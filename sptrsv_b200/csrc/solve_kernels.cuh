@@ -460,6 +460,107 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstr
     }
 }
 
+// WAVE schedule (see strip.cu): CTA c takes line groups c, c + gridDim, ...;
+// warp w of the CTA solves line w of the group chunk by chunk (the same
+// chunk arithmetic as STRIP).  The group's x values live in shared memory
+// (filled with the sentinel first): a column inside the group is encoded
+// ~(column - first row of the group) and polled there, so the wait on the
+// line above is a shared-memory hop; other columns (the group's first line
+// on the previous group, far planes) are polled in x.  After a group every
+// warp meets at a CTA barrier before the shared copy is reused; a warp
+// whose wait ran out raises a CTA flag there and the CTA leaves.
+template <typename V>
+struct WaveMat {
+    StripMat<V> c;                 // slot arrays (sptr unused)
+    const int* __restrict__ runc;  // first chunk of each run
+    const int* __restrict__ grun;  // first run of each group
+    const int* __restrict__ grow;  // first row of each group
+};
+
+template <typename V, typename T, typename BT, int OUT>
+__global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroups, const BT* __restrict__ b, T* x,
+                                                        double* x64, DevStatus* st, unsigned long long budget,
+                                                        unsigned backoff)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int abort_flag;
+    const unsigned FULL = 0xffffffffu;
+    volatile T* xs = reinterpret_cast<volatile T*>(smem_raw);
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const StripMat<V>& m = w.c;
+    if (threadIdx.x == 0) abort_flag = 0;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const int r0 = __ldg(w.grow + g), nr = __ldg(w.grow + g + 1) - r0;
+        for (int t = threadIdx.x; t < nr; t += blockDim.x) xs[t] = sentinel_value<T>();
+        __syncthreads();
+        const int run = __ldg(w.grun + g) + wib;
+        bool failed = false;
+        if (run < __ldg(w.grun + g + 1)) {
+            const int q0 = __ldg(w.runc + run), q1 = __ldg(w.runc + run + 1);
+            StripMeta<T> m0, m1;
+            StripEnt<T> e0;
+            strip_meta<V, T>(m0, m, q0 * 32 + lane);
+            strip_ent<V, T, BT>(e0, m0, m, b);
+            if (q0 + 1 < q1) strip_meta<V, T>(m1, m, (q0 + 1) * 32 + lane);
+            for (int q = q0; q < q1 && !failed; q++) {
+                const StripMeta<T> md = m0;
+                const StripEnt<T> en = e0;
+                if (q + 1 < q1) {
+                    m0 = m1;
+                    strip_ent<V, T, BT>(e0, m0, m, b);
+                    if (q + 2 < q1) strip_meta<V, T>(m1, m, (q + 2) * 32 + lane);
+                }
+                const int ec = md.e1 - md.e0;
+                T acc = en.b;
+                const int rounds = __reduce_max_sync(FULL, ec);
+                for (int j = 0; j < rounds; j += kStripU) {
+                    const int nh = min(kStripU, ec - j);
+                    int cc[kStripU];
+                    T vv[kStripU], xv[kStripU];
+#pragma unroll
+                    for (int u = 0; u < kStripU; u++) {
+                        cc[u] = en.cc[u];
+                        vv[u] = en.vv[u];
+                        if (j > 0) {
+                            cc[u] = 0;
+                            vv[u] = 0;
+                            if (u < nh) {
+                                cc[u] = __ldg(m.ecol + md.e0 + j + u);
+                                vv[u] = (T)__ldg(m.ev + md.e0 + j + u);
+                            }
+                        }
+                    }
+                    if (!warp_wait_n<true, kStripU, T>(nh, cc, x, xs, xv, st, budget, backoff, md.row)) {
+                        failed = true;
+                        break;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kStripU; u++)
+                        if (u < nh) acc -= vv[u] * xv[u];
+                }
+                if (failed) break;
+                T a = acc * md.piv, bb = -md.lsub * md.piv;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T ap = __shfl_up_sync(FULL, a, d), bp = __shfl_up_sync(FULL, bb, d);
+                    if (lane >= d) {
+                        a = a + bb * ap;
+                        bb = bb * bp;
+                    }
+                }
+                const T xi = publishable(a);
+                if (md.row >= 0) {
+                    xs[md.row - r0] = xi;
+                    publish<T, OUT>(x, x64, md.row, xi);
+                }
+            }
+        }
+        if (failed && lane == 0) abort_flag = 1;
+        __syncthreads();
+        if (abort_flag) return;
+    }
+}
+
 // Natural-order chunks (the plan's SIMPLE schedule): warp task t covers the
 // natural rows [t*R, t*R+R) and solves them one after another with all 32
 // lanes striding each row's elements.  A dependency inside the chunk was

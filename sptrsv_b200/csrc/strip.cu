@@ -142,6 +142,29 @@ __global__ void k_strip_fill(SptLayout l, const int* __restrict__ inv, const int
     }
 }
 
+// WAVE entries (natural chunk order): a column inside the row's group is
+// encoded as ~(column - first row of the group), its value is then read
+// from the CTA's shared-memory copy.
+__global__ void k_wave_fill(SptLayout l, const int* __restrict__ inv, const int* __restrict__ row, int nslots,
+                            const int* __restrict__ rchunk, const int* __restrict__ chunk_g0,
+                            const int* __restrict__ pe, int* __restrict__ ecol, double* __restrict__ ev64,
+                            float* __restrict__ ev32)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nslots; t += gridDim.x * blockDim.x) {
+        const int i = row[t];
+        if (i < 0) continue;
+        const int g0 = chunk_g0[rchunk[i]];
+        const int s = l.ptr[inv[i]];
+        const int o = pe[t], cnt = pe[t + 1] - o;
+        for (int k = 0; k < cnt; k++) {
+            const int c = l.col[s + k];
+            ecol[o + k] = c >= g0 ? ~(c - g0) : c;
+            ev64[o + k] = l.val64[s + k];
+            ev32[o + k] = l.val32[s + k];
+        }
+    }
+}
+
 }  // namespace
 
 void strip_free(StripLayout& t)
@@ -150,6 +173,101 @@ void strip_free(StripLayout& t)
     cudaFree(t.lsub32); cudaFree(t.di64); cudaFree(t.di32); cudaFree(t.sptr);
     t = StripLayout{};
 }
+
+void wave_free(WaveLayout& w)
+{
+    cudaFree(w.row); cudaFree(w.pe); cudaFree(w.ecol); cudaFree(w.ev64); cudaFree(w.ev32); cudaFree(w.lsub64);
+    cudaFree(w.lsub32); cudaFree(w.di64); cudaFree(w.di32); cudaFree(w.runc); cudaFree(w.grun); cudaFree(w.grow);
+    w = WaveLayout{};
+}
+
+namespace {
+
+// The chunk cut and the per-row data both layouts start from.
+struct Chunks {
+    std::vector<int> cstart, rchunk;   // host: first row of each chunk (+ n), chunk of each row
+    std::vector<unsigned char> linked; // host: chunk continues the previous chunk's run
+    int nch = 0, m = 0;                // chunks, entries before their rows' chunks
+    int *d_rchunk = nullptr, *d_cstart = nullptr, *eptr = nullptr;
+    double *nlsub = nullptr, *ndi = nullptr;
+    float* ndi32 = nullptr;
+    void release()
+    {
+        cudaFree(d_rchunk); cudaFree(d_cstart); cudaFree(eptr); cudaFree(nlsub); cudaFree(ndi); cudaFree(ndi32);
+        d_rchunk = d_cstart = eptr = nullptr;
+        nlsub = ndi = nullptr;
+        ndi32 = nullptr;
+    }
+};
+
+// Cuts the chunks, checks the structure (SPTRSV_ERR_UNSUPPORTED otherwise)
+// and fills the per-natural-row arrays.  On error everything is released.
+int chunk_analysis(sptrsv_plan_s* p, Chunks& c, cudaStream_t s)
+{
+    const int n = p->n;
+    unsigned char* brk = nullptr;
+    int *ecnt = nullptr, *flag = nullptr, *scr = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(brk); cudaFree(ecnt); cudaFree(flag); cudaFree(scr);
+    };
+    auto fail = [&](int code) {
+        cleanup();
+        c.release();
+        return code;
+    };
+#define CCHK(call)                                                \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
+    } while (0)
+    // chunks: a new one at every row that does not depend on the row before
+    // it, and after 32 rows
+    CCHK(dalloc(&brk, n));
+    k_strip_breaks<<<grid_for(n, 256), 256, 0, s>>>(p->lev, p->inv, n, brk);
+    CCHK(cudaGetLastError());
+    std::vector<unsigned char> hbrk(n);
+    CCHK(cudaMemcpy(hbrk.data(), brk, (size_t)n, cudaMemcpyDeviceToHost));
+    c.cstart.clear();
+    c.linked.clear();
+    c.rchunk.assign(n, 0);
+    for (int i = 0; i < n; i++) {
+        if (hbrk[i] || i - c.cstart.back() == 32) {
+            c.cstart.push_back(i);
+            c.linked.push_back((unsigned char)!hbrk[i]);
+        }
+        c.rchunk[i] = (int)c.cstart.size() - 1;
+    }
+    c.nch = (int)c.cstart.size();
+    c.cstart.push_back(n);
+    CCHK(dalloc(&c.d_rchunk, n));
+    CCHK(dalloc(&c.d_cstart, c.nch + 1));
+    CCHK(cudaMemcpy(c.d_rchunk, c.rchunk.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+    CCHK(cudaMemcpy(c.d_cstart, c.cstart.data(), sizeof(int) * ((size_t)c.nch + 1), cudaMemcpyHostToDevice));
+    // per natural row: entries before the chunk, L(i, i-1), 1/diagonal
+    CCHK(dalloc(&ecnt, (long long)n + 1));
+    CCHK(dalloc(&flag, 1));
+    CCHK(dalloc(&c.nlsub, n));
+    CCHK(dalloc(&c.ndi, n));
+    CCHK(dalloc(&c.ndi32, n));
+    CCHK(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    CCHK(cudaMemsetAsync(ecnt + n, 0, sizeof(int), s));
+    k_strip_rows<<<grid_for(n, 256), 256, 0, s>>>(p->lev, p->inv, n, c.d_rchunk, c.d_cstart, ecnt, c.nlsub, c.ndi,
+                                                  c.ndi32, flag);
+    CCHK(cudaGetLastError());
+    int hflag = 0;
+    CCHK(cudaMemcpy(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hflag) return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "strip schedule: a row depends on a row of its own "
+                                                              "chunk other than the one before it"));
+    CCHK(dalloc(&c.eptr, (long long)n + 1));
+    CCHK(dalloc(&scr, scan_scratch_ints((long long)n + 1)));
+    CCHK(scan_exclusive(ecnt, c.eptr, (long long)n + 1, scr, s));
+    CCHK(cudaMemcpy(&c.m, c.eptr + n, sizeof(int), cudaMemcpyDeviceToHost));
+#undef CCHK
+    cleanup();
+    return 0;
+}
+
+}  // namespace
 
 int build_strip_layout(sptrsv_plan_s* p, int R)
 {
@@ -160,15 +278,22 @@ int build_strip_layout(sptrsv_plan_s* p, int R)
     const int W = 2 * R;
     cudaStream_t s = 0;
     StripLayout t{};
-    int *ecnt = nullptr, *eptr = nullptr, *ext = nullptr, *flag = nullptr, *scr = nullptr, *d_strip_of = nullptr,
-        *d_pos = nullptr, *d_chunk_at = nullptr, *scnt = nullptr, *d_rchunk = nullptr, *d_cstart = nullptr;
-    double *nlsub = nullptr, *ndi = nullptr;
-    float* ndi32 = nullptr;
-    unsigned char* brk = nullptr;
+    Chunks ch;
+    {
+        int e = chunk_analysis(p, ch, s);
+        if (e) return e;
+    }
+    const int nch = ch.nch, nslots = nch * 32, m = ch.m;
+    const std::vector<int>& cstart = ch.cstart;
+    const std::vector<int>& rchunk = ch.rchunk;
+    const std::vector<unsigned char>& linked = ch.linked;
+    int *ext = nullptr, *flag = nullptr, *scr = nullptr, *d_strip_of = nullptr, *d_pos = nullptr,
+        *d_chunk_at = nullptr, *scnt = nullptr;
+    int* eptr = ch.eptr;
     auto cleanup = [&]() {
-        cudaFree(ecnt); cudaFree(eptr); cudaFree(ext); cudaFree(flag); cudaFree(scr); cudaFree(d_strip_of);
-        cudaFree(d_pos); cudaFree(d_chunk_at); cudaFree(scnt); cudaFree(d_rchunk); cudaFree(d_cstart);
-        cudaFree(nlsub); cudaFree(ndi); cudaFree(ndi32); cudaFree(brk);
+        cudaFree(ext); cudaFree(flag); cudaFree(scr); cudaFree(d_strip_of); cudaFree(d_pos); cudaFree(d_chunk_at);
+        cudaFree(scnt);
+        ch.release();
     };
     auto fail = [&](int code) {
         cleanup();
@@ -180,50 +305,10 @@ int build_strip_layout(sptrsv_plan_s* p, int R)
         cudaError_t e_ = (call);                                  \
         if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
     } while (0)
-    // 1. chunks: a new one at every row that does not depend on the row
-    //    before it, and after 32 rows
-    SCHK(dalloc(&brk, n));
-    k_strip_breaks<<<grid_for(n, 256), 256, 0, s>>>(p->lev, p->inv, n, brk);
-    SCHK(cudaGetLastError());
-    std::vector<unsigned char> hbrk(n);
-    SCHK(cudaMemcpy(hbrk.data(), brk, (size_t)n, cudaMemcpyDeviceToHost));
-    std::vector<int> cstart, rchunk(n);
-    std::vector<unsigned char> linked;  // chunk continues the previous one's run
-    for (int i = 0; i < n; i++) {
-        if (hbrk[i] || i - cstart.back() == 32) {
-            cstart.push_back(i);
-            linked.push_back((unsigned char)!hbrk[i]);
-        }
-        rchunk[i] = (int)cstart.size() - 1;
-    }
-    const int nch = (int)cstart.size();
-    cstart.push_back(n);
-    const int nslots = nch * 32;
-    SCHK(dalloc(&d_rchunk, n));
-    SCHK(dalloc(&d_cstart, nch + 1));
-    SCHK(cudaMemcpy(d_rchunk, rchunk.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
-    SCHK(cudaMemcpy(d_cstart, cstart.data(), sizeof(int) * ((size_t)nch + 1), cudaMemcpyHostToDevice));
-    // 2. per natural row: entries before the chunk, L(i, i-1), 1/diagonal
-    SCHK(dalloc(&ecnt, (long long)n + 1));
     SCHK(dalloc(&flag, 1));
-    SCHK(dalloc(&nlsub, n));
-    SCHK(dalloc(&ndi, n));
-    SCHK(dalloc(&ndi32, n));
     SCHK(cudaMemsetAsync(flag, 0, sizeof(int), s));
-    SCHK(cudaMemsetAsync(ecnt + n, 0, sizeof(int), s));
-    k_strip_rows<<<grid_for(n, 256), 256, 0, s>>>(p->lev, p->inv, n, d_rchunk, d_cstart, ecnt, nlsub, ndi, ndi32,
-                                                  flag);
-    SCHK(cudaGetLastError());
-    int hflag = 0;
-    SCHK(cudaMemcpy(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (hflag) return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "strip schedule: a row depends on a row of its own "
-                                                              "chunk other than the one before it"));
-    // 3. their columns on the host: chunk dependencies
-    SCHK(dalloc(&eptr, (long long)n + 1));
     SCHK(dalloc(&scr, scan_scratch_ints((long long)nslots + 1)));
-    SCHK(scan_exclusive(ecnt, eptr, (long long)n + 1, scr, s));
-    int m = 0;
-    SCHK(cudaMemcpy(&m, eptr + n, sizeof(int), cudaMemcpyDeviceToHost));
+    // 3. their columns on the host: chunk dependencies
     SCHK(dalloc(&ext, m));
     k_strip_extcols<<<grid_for(n, 256), 256, 0, s>>>(p->lev, p->inv, n, eptr, ext);
     SCHK(cudaGetLastError());
@@ -294,17 +379,18 @@ int build_strip_layout(sptrsv_plan_s* p, int R)
     SCHK(dalloc(&t.di64, nslots));
     SCHK(dalloc(&t.di32, nslots));
     SCHK(cudaMemsetAsync(scnt + nslots, 0, sizeof(int), s));
-    k_strip_slots<<<grid_for(nslots, 256), 256, 0, s>>>(d_chunk_at, d_cstart, nslots, eptr, nlsub, ndi, ndi32, t.row,
-                                                        scnt, t.lsub64, t.lsub32, t.di64, t.di32);
+    k_strip_slots<<<grid_for(nslots, 256), 256, 0, s>>>(d_chunk_at, ch.d_cstart, nslots, eptr, ch.nlsub, ch.ndi,
+                                                        ch.ndi32, t.row, scnt, t.lsub64, t.lsub32, t.di64, t.di32);
     SCHK(cudaGetLastError());
     SCHK(dalloc(&t.pe, (long long)nslots + 1));
     SCHK(scan_exclusive(scnt, t.pe, (long long)nslots + 1, scr, s));
     SCHK(dalloc(&t.ecol, m));
     SCHK(dalloc(&t.ev64, m));
     SCHK(dalloc(&t.ev32, m));
-    k_strip_fill<<<grid_for(nslots, 256), 256, 0, s>>>(p->lev, p->inv, t.row, nslots, d_rchunk, d_cstart, t.pe,
+    k_strip_fill<<<grid_for(nslots, 256), 256, 0, s>>>(p->lev, p->inv, t.row, nslots, ch.d_rchunk, ch.d_cstart, t.pe,
                                                        d_strip_of, d_pos, W, t.ecol, t.ev64, t.ev32, flag);
     SCHK(cudaGetLastError());
+    int hflag = 0;
     SCHK(cudaMemcpy(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (hflag) return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "strip schedule: a dependency inside a strip does not "
                                                               "come earlier in its wavefront order"));
@@ -315,6 +401,93 @@ int build_strip_layout(sptrsv_plan_s* p, int R)
     cleanup();
     p->strip = t;
     p->row_strip_R = R;
+    return 0;
+}
+
+int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows)
+{
+    if (p->wave.row && p->wave.G == G) return 0;
+    wave_free(p->wave);
+    cudaStream_t s = 0;
+    WaveLayout w{};
+    Chunks ch;
+    {
+        int e = chunk_analysis(p, ch, s);
+        if (e) return e;
+    }
+    const int nch = ch.nch, nslots = nch * 32, m = ch.m;
+    int *d_ident = nullptr, *d_g0 = nullptr, *scnt = nullptr, *scr = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_ident); cudaFree(d_g0); cudaFree(scnt); cudaFree(scr);
+        ch.release();
+    };
+    auto fail = [&](int code) {
+        cleanup();
+        wave_free(w);
+        return code;
+    };
+#define WCHK(call)                                                \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
+    } while (0)
+    // runs (grid lines) and groups of G runs
+    std::vector<int> run0;
+    for (int q = 0; q < nch; q++)
+        if (q == 0 || !ch.linked[q]) run0.push_back(q);
+    const int nruns = (int)run0.size();
+    run0.push_back(nch);
+    const int ngroups = (nruns + G - 1) / G;
+    std::vector<int> grun(ngroups + 1), grow(ngroups + 1), g0(nch), ident(nch);
+    int cap = 0;
+    for (int g = 0; g <= ngroups; g++) {
+        grun[g] = std::min(nruns, g * G);
+        grow[g] = ch.cstart[run0[grun[g]]];
+        if (g > 0) cap = std::max(cap, grow[g] - grow[g - 1]);
+    }
+    if (cap > max_rows)
+        return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "wave schedule: %d lines of the matrix hold %d rows, more than "
+                                                      "the %d that fit shared memory", G, cap, max_rows));
+    for (int g = 0; g < ngroups; g++)
+        for (int q = run0[grun[g]]; q < run0[grun[g + 1]]; q++) g0[q] = grow[g];
+    for (int q = 0; q < nch; q++) ident[q] = q;
+    WCHK(dalloc(&w.runc, nruns + 1));
+    WCHK(dalloc(&w.grun, ngroups + 1));
+    WCHK(dalloc(&w.grow, ngroups + 1));
+    WCHK(dalloc(&d_ident, nch));
+    WCHK(dalloc(&d_g0, nch));
+    WCHK(cudaMemcpy(w.runc, run0.data(), sizeof(int) * (size_t)(nruns + 1), cudaMemcpyHostToDevice));
+    WCHK(cudaMemcpy(w.grun, grun.data(), sizeof(int) * (size_t)(ngroups + 1), cudaMemcpyHostToDevice));
+    WCHK(cudaMemcpy(w.grow, grow.data(), sizeof(int) * (size_t)(ngroups + 1), cudaMemcpyHostToDevice));
+    WCHK(cudaMemcpy(d_ident, ident.data(), sizeof(int) * (size_t)nch, cudaMemcpyHostToDevice));
+    WCHK(cudaMemcpy(d_g0, g0.data(), sizeof(int) * (size_t)nch, cudaMemcpyHostToDevice));
+    // slots and entries in natural chunk order
+    WCHK(dalloc(&w.row, nslots));
+    WCHK(dalloc(&scnt, (long long)nslots + 1));
+    WCHK(dalloc(&w.lsub64, nslots));
+    WCHK(dalloc(&w.lsub32, nslots));
+    WCHK(dalloc(&w.di64, nslots));
+    WCHK(dalloc(&w.di32, nslots));
+    WCHK(cudaMemsetAsync(scnt + nslots, 0, sizeof(int), s));
+    k_strip_slots<<<grid_for(nslots, 256), 256, 0, s>>>(d_ident, ch.d_cstart, nslots, ch.eptr, ch.nlsub, ch.ndi,
+                                                        ch.ndi32, w.row, scnt, w.lsub64, w.lsub32, w.di64, w.di32);
+    WCHK(cudaGetLastError());
+    WCHK(dalloc(&scr, scan_scratch_ints((long long)nslots + 1)));
+    WCHK(dalloc(&w.pe, (long long)nslots + 1));
+    WCHK(scan_exclusive(scnt, w.pe, (long long)nslots + 1, scr, s));
+    WCHK(dalloc(&w.ecol, m));
+    WCHK(dalloc(&w.ev64, m));
+    WCHK(dalloc(&w.ev32, m));
+    k_wave_fill<<<grid_for(nslots, 256), 256, 0, s>>>(p->lev, p->inv, w.row, nslots, ch.d_rchunk, d_g0, w.pe, w.ecol,
+                                                      w.ev64, w.ev32);
+    WCHK(cudaGetLastError());
+    WCHK(cudaStreamSynchronize(s));
+#undef WCHK
+    w.ngroups = ngroups;
+    w.G = G;
+    w.cap = cap;
+    cleanup();
+    p->wave = w;
     return 0;
 }
 

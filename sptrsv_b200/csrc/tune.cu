@@ -2,11 +2,12 @@
 // schedule prediction.
 //
 // 24 classes = 4 groups x 6 parameter presets.  The natural-order group holds
-// SIMPLE with 1 and 32 rows per task and STRIP with 1, 2, 8 and 16 grid lines
-// per warp (STRIP applies only to matrices with its chunk structure; elsewhere
-// its classes fail to set and are skipped).  For ORDER the preset is rows per
-// warp (1..32, i.e. 32..1 lanes per row — the reference's six tile sizes,
-// analysis_csr.cu:84-102).  MULTIROW takes lanes per row from the analysis
+// SIMPLE with 1 and 32 rows per task, STRIP with one grid line per warp and
+// WAVE with 4, 8 and 16 grid lines per CTA (STRIP and WAVE apply only to
+// matrices with their chunk structure, WAVE only where a line group fits
+// shared memory; elsewhere those classes fail to set and are skipped).  For
+// ORDER the preset is rows per warp (1..32, i.e. 32..1 lanes per row — the
+// reference's six tile sizes, analysis_csr.cu:84-102).  MULTIROW takes lanes per row from the analysis
 // map, so its presets vary the polling back-off and the number of resident
 // warps.  CLUSTER presets vary band height, cluster size and lanes per row.
 #include <algorithm>
@@ -30,10 +31,11 @@ int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
 {
     if (!s || cls < 0 || cls >= SPTRSV_N_CLASSES) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule_from_class: bad class");
     static const int rpw[6] = {1, 2, 4, 8, 16, 32};
-    // natural-order group: SIMPLE with 1 and 32 rows per task; STRIP with
-    // 1, 2, 8, 16 grid lines per warp in between
-    static const int strip_r[6] = {0, 1, 2, 8, 16, 0};
-    static const int strip_bw[6] = {0, 2, 4, 4, 8, 0};
+    // natural-order group: SIMPLE with 1 and 32 rows per task; between them
+    // STRIP with one grid line per warp and WAVE with 4, 8, 16 lines per CTA
+    static const int nat_v[6] = {SPTRSV_VAR_SIMPLE, SPTRSV_VAR_STRIP, SPTRSV_VAR_WAVE, SPTRSV_VAR_WAVE,
+                                 SPTRSV_VAR_WAVE, SPTRSV_VAR_SIMPLE};
+    static const int nat_bw[6] = {8, 2, 4, 8, 16, 8};
     // MULTIROW presets: block warps, back-off ns, resident warps per SM
     static const int mr[6][3] = {{8, 0, 0}, {8, 200, 0}, {8, 1000, 0}, {4, 0, 16}, {8, 200, 32}, {16, 0, 0}};
     // CLUSTER presets: band levels, cluster rows, rows per warp, block warps
@@ -50,10 +52,10 @@ int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
     s->ir_max_iters = 2;
     s->band_levels = 64;
     s->cluster_rows = 4096;
-    if (v == SPTRSV_VAR_SIMPLE && strip_r[j]) {
-        s->variant = SPTRSV_VAR_STRIP;
-        s->rows_per_warp = strip_r[j];
-        s->block_warps = strip_bw[j];
+    if (v == SPTRSV_VAR_SIMPLE && nat_v[j] != SPTRSV_VAR_SIMPLE) {
+        s->variant = nat_v[j];
+        s->rows_per_warp = 1;
+        s->block_warps = nat_bw[j];
     } else if (v == SPTRSV_VAR_SIMPLE || v == SPTRSV_VAR_ORDER) {
         s->rows_per_warp = rpw[j];
     } else if (v == SPTRSV_VAR_MULTIROW) {
@@ -154,7 +156,7 @@ int sptrsv_plan_select_schedule(sptrsv_plan_t p, sptrsv_mlp_t M, const sp_mat_t*
     int e = sptrsv_features(L, info, f);
     if (e) return e;
     // classes in order of predicted time; the first one that applies to
-    // this matrix (a STRIP class needs its chunk structure) is set
+    // this matrix (STRIP and WAVE classes need its chunk structure) is set
     float out[SPTRSV_N_CLASSES];
     e = sptrsv_mlp_forward_host(M, f, 1, out);
     if (e) return e;

@@ -17,7 +17,7 @@ from ._lib import AnalysisInfo, Schedule, SpMat
 N_CLASSES = 24
 N_FEATURES = 12
 N_PARAMS = 6552
-VARIANT_NAMES = ["simple", "order", "multirow", "cluster", "strip"]
+VARIANT_NAMES = ["simple", "order", "multirow", "cluster", "strip", "wave"]
 FEATURE_NAMES = ["log2_n", "log2_nnz", "nnz_per_row", "log2_nlevs", "log2_mean_level_width",
                  "log2_max_level_width", "q25_offdiag", "q50_offdiag", "q90_offdiag", "q99_offdiag",
                  "log2_1p_max_offdiag", "frac_diag_only"]
@@ -42,6 +42,8 @@ def class_name(cls: int) -> str:
         return f"{v}/rpw{s.rows_per_warp}"
     if s.variant == 4:
         return f"{v}/R{s.rows_per_warp}-bw{s.block_warps}"
+    if s.variant == 5:
+        return f"{v}/G{s.block_warps}"
     if s.variant == 2:
         return f"{v}/bw{s.block_warps}-bo{s.backoff_ns}-wps{s.warps_per_sm}"
     return f"{v}/H{s.band_levels}-B{s.cluster_rows}-rpw{s.rows_per_warp}-bw{s.block_warps}"

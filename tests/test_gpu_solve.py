@@ -292,15 +292,18 @@ def test_strip_schedule_fp64_and_ir(torch_cuda, name):
     plan = S.Plan(L, info)
     db = torch.from_numpy(b).cuda()
     dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
-    for r, bw in ((1, 4), (2, 2), (4, 4), (8, 4), (16, 4), (32, 2)):
-        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=bw, ir_max_iters=2)
+    scheds = [dict(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=bw)
+              for r, bw in ((1, 4), (2, 2), (4, 4), (8, 4), (16, 4), (32, 2))]
+    scheds += [dict(variant=S._lib.VAR_WAVE, block_warps=g) for g in (2, 4, 8, 16)]
+    for sc in scheds:
+        plan.set_schedule(ir_max_iters=2, **sc)
         for rep in range(2):
             plan.solve_f64(db, dx)
             S.sync_status()
-            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, (r, bw, rep)
+            assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, (sc, rep)
         plan.solve_ir(db, dx)
         S.sync_status()
-        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", r, bw)
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, ("ir", sc)
     # new values, same pattern: the strip copy is rebuilt
     m2 = gen.HostCsr(m.rowptr, m.colidx, m.val * 1.5)
     L2 = S.allocate_memory(m2.rowptr, m2.colidx, m2.val, m2.n)
@@ -320,15 +323,38 @@ def test_strip_schedule_rejects_other_structures(torch_cuda, name):
     m = gen.banded(5000, 64, 4, 8, seed=1) if name == "banded" else gen.zipf(5000, 1.5, 64, seed=1)
     L, info = _setup(S, m, S.MULTIROW)
     plan = S.Plan(L, info)
+    for v in (S._lib.VAR_STRIP, S._lib.VAR_WAVE):
+        with pytest.raises(S.SptrsvError) as ei:
+            plan.set_schedule(variant=v, rows_per_warp=4, block_warps=4)
+        assert ei.value.code == S._lib.SPTRSV_ERR_UNSUPPORTED
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+def test_wave_schedule_rejects_groups_beyond_shared_memory(torch_cuda):
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.grid2d(10000, 20, seed=1)  # 16 lines of 10,000 rows do not fit shared memory; 2 lines do
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
     with pytest.raises(S.SptrsvError) as ei:
-        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=4, block_warps=4)
+        plan.set_schedule(variant=S._lib.VAR_WAVE, block_warps=16)
     assert ei.value.code == S._lib.SPTRSV_ERR_UNSUPPORTED
+    xt = gen.vector(m.n, "uniform", seed=2)
+    b = m.matvec(xt)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty_like(db)
+    plan.set_schedule(variant=S._lib.VAR_WAVE, block_warps=2)
+    plan.solve_f64(db, dx)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), O.solve(m.rowptr, m.colidx, m.val, b)) <= TOL
     plan.close()
     S.free_device_analysis(L, info)
 
 
 def test_selector_skips_classes_that_do_not_apply(torch_cuda):
-    """A network that ranks a STRIP class first: on a grid it is taken, on a
+    """A network that ranks a WAVE class first: on a grid it is taken, on a
     banded matrix the next class in predicted order is."""
     import sptrsv_b200 as S
     from sptrsv_b200 import select as SEL
@@ -336,7 +362,7 @@ def test_selector_skips_classes_that_do_not_apply(torch_cuda):
     net = SEL.Mlp(seed=1)
     p = np.zeros(SEL.N_PARAMS, np.float32)
     b3 = np.arange(SEL.N_CLASSES, dtype=np.float32)
-    b3[2] = -10.0  # a STRIP class first, then class 0, 1, 3, ...
+    b3[2] = -10.0  # a WAVE class first, then class 0, 1, 3, ...
     p[-SEL.N_CLASSES:] = b3
     net.set_params(p)
     net.set_normalization(np.zeros(SEL.N_FEATURES, np.float32), np.ones(SEL.N_FEATURES, np.float32))
@@ -361,10 +387,12 @@ def test_strip_full_size_grid(torch_cuda):
     plan = S.Plan(L, info)
     db = torch.from_numpy(b).cuda()
     dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
-    for r in (4, 8, 16, 32):
-        plan.set_schedule(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=2 if r == 32 else 4)
+    scheds = [dict(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=2 if r == 32 else 4) for r in (1, 4, 32)]
+    scheds += [dict(variant=S._lib.VAR_WAVE, block_warps=g) for g in (4, 8)]
+    for sc in scheds:
+        plan.set_schedule(**sc)
         plan.solve_f64(db, dx)
         S.sync_status()
-        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, r
+        assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, sc
     plan.close()
     S.free_device_analysis(L, info)
