@@ -144,6 +144,8 @@ __device__ __forceinline__ void load_slot(Slot<T>& s, const M& m, int base, int 
     }
 }
 
+constexpr int kSlotU = 4;
+
 // Runs one task: each lane takes its row's elements in rounds (lane sl of a
 // row takes elements sl, sl+L, ...), the warp waits for a round's
 // dependencies together, then rows reduce under their segment mask and
@@ -167,18 +169,32 @@ __device__ __forceinline__ bool run_slot(const Slot<T>& s, const M& m, int lane,
     const int mine = s.act ? max(0, (s.q.e - s.q.s - sl + L - 1) / L) : 0;
     const int rounds = __reduce_max_sync(0xffffffffu, mine);
     int p = s.q.s + sl;
-    int c = s.c0;
-    T v = s.v0;
-    for (int j = 0; j < rounds; j++) {
-        const bool have = j < mine;
-        if (have && j > 0) {
-            c = m.c(p);
-            v = (T)m.v(p);
-        }
+    if (rounds > 0) {  // the first element was loaded with the task
+        const bool have = 0 < mine;
         T xv = 0;
-        if (!warp_wait<SMEM, T>(have, c, x, xs, xv, st, budget, backoff, s.q.r)) return true;
-        if (have) acc -= v * xv;
+        if (!warp_wait<SMEM, T>(have, s.c0, x, xs, xv, st, budget, backoff, s.q.r)) return true;
+        if (have) acc -= s.v0 * xv;
         p += L;
+    }
+    // long rows: kSlotU further elements per lane per wait, loads back to back
+    for (int j = 1; j < rounds; j += kSlotU) {
+        const int nh = min(kSlotU, mine - j);
+        int cc[kSlotU];
+        T vv[kSlotU], xv[kSlotU];
+#pragma unroll
+        for (int u = 0; u < kSlotU; u++) {
+            cc[u] = 0;
+            vv[u] = 0;
+            if (u < nh) {
+                cc[u] = m.c(p + u * L);
+                vv[u] = (T)m.v(p + u * L);
+            }
+        }
+        if (!warp_wait_n<SMEM, kSlotU, T>(nh, cc, x, xs, xv, st, budget, backoff, s.q.r)) return true;
+#pragma unroll
+        for (int u = 0; u < kSlotU; u++)
+            if (u < nh) acc -= vv[u] * xv[u];
+        p += kSlotU * L;
     }
     for (int o = L >> 1; o >= 1; o >>= 1) acc += __shfl_down_sync(smask, acc, o, L);
     if (s.act && sl == 0) {
