@@ -56,6 +56,12 @@ __device__ __forceinline__ int ld_relaxed(const int* p)
     asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ void st_relaxed(double* p, double v)
 {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v))
@@ -235,6 +241,35 @@ __device__ __forceinline__ bool warp_wait_n(int nh, const I (&c)[U], const T* x,
         }
         if (!__any_sync(0xffffffffu, pend != 0)) return true;
     }
+}
+
+// Warp-convergent bounded wait until *flag == want for every lane with
+// need set (acquire: later loads see what was written before the flag).
+// Same contract as warp_wait.
+__device__ __forceinline__ bool warp_wait_flag(bool need, const int* flag, int want, DevStatus* st,
+                                               unsigned long long budget, int row)
+{
+    unsigned long long t0 = 0;
+    unsigned it = 0;
+    bool pending = need && ld_acquire(flag) != want;
+    while (__any_sync(0xffffffffu, pending)) {
+        ++it;
+        if ((it & 63u) == 0) {
+            int stop = 0;
+            if ((threadIdx.x & 31) == 0) {
+                unsigned long long now = global_ns();
+                if (t0 == 0) t0 = now;
+                if (ld_relaxed(&st->code) != 0) stop = 1;
+                else if (now - t0 > budget) {
+                    report(st, SPTRSV_ERR_TIMEOUT, row);
+                    stop = 1;
+                }
+            }
+            if (__shfl_sync(0xffffffffu, stop, 0)) return false;
+        }
+        if (pending) pending = ld_acquire(flag) != want;
+    }
+    return true;
 }
 
 template <typename T>

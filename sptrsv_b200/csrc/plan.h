@@ -90,6 +90,17 @@ struct sptrsv_plan_s {
     StripLayout strip;           // STRIP layout (built on demand)
     int row_strip_R = 0;         // R the strip layout was built for (0: none)
     WaveLayout wave;             // WAVE layout (built on demand)
+    // streamed host solves (WAVE, FP64): b copied in segments on a side
+    // stream while the kernel runs, one flag word per segment
+    int* bflag = nullptr;        // [nseg] epoch of the last copy of each segment
+    int nseg = 0;
+    int* epochs = nullptr;       // pinned host table: epochs[e] = e, the flag values' source
+    int epoch = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_copied = nullptr;
+    const int* launch_bflag = nullptr;  // set only during a streamed launch
+    int launch_epoch = 0;
+    double* launch_hx = nullptr;
     float* w32a = nullptr;
     float* w32b = nullptr;
     int cap_rhs = 0;

@@ -1,6 +1,7 @@
 // solve.cu — host side of the solves: the reference entry points
 // (header/solver.h:5-7) over the caller's CSR, and the plan API over the
 // plan's layouts (FP64, FP32 + FP64 refinement, 1-32 RHS).
+#include <algorithm>
 #include <cstring>
 
 #include "internal.h"
@@ -18,6 +19,9 @@ bool pow2_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 
 
 // Rows of one WAVE line group: their FP64 x values fill the CTA's shared memory.
 constexpr int kWaveMaxRows = 200 * 1024 / 8;
+// Streamed host solves: rows per copied segment of b (1 MiB of doubles; a
+// multiple of 16 rows, so no 128-byte line of b spans two segments).
+constexpr int kStreamSegRows = 1 << 17;
 
 // Shared memory of the STRIP kernel: per warp a ring of 2R chunks of 32 values.
 size_t strip_smem_bytes(const sptrsv_schedule_t* s, size_t elem)
@@ -113,6 +117,8 @@ int solve_reference(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b, d
 
 // ---- plan ----------------------------------------------------------------------
 
+int plan_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s);
+
 namespace {
 
 __global__ void k_plan_rows(const int* __restrict__ rowptr, const int* __restrict__ iorder, int n,
@@ -164,6 +170,73 @@ void plan_free_arrays(sptrsv_plan_s* p)
     for (int j = 0; j < 6; j++) cudaFree(p->ord_tasks[j]);
     cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
     cudaFree(p->w32a); cudaFree(p->w32b); cudaFree(p->hb); cudaFree(p->hx);
+    cudaFree(p->bflag);
+    if (p->epochs) cudaFreeHost(p->epochs);
+    if (p->ev_start) cudaEventDestroy(p->ev_start);
+    if (p->ev_copied) cudaEventDestroy(p->ev_copied);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+}
+
+// Pinned host memory the device can address directly (its device pointer),
+// else nullptr.
+void* mapped_host(const void* h)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    return a.devicePointer;
+}
+
+// The streamed host solve of a WAVE plan (FP64, one right-hand side, pinned
+// host b and x): b goes to the device in segments on a side stream, each
+// segment followed by a 4-byte copy of the call's epoch into its flag word,
+// while the solve kernel already runs; the kernel waits for a segment's flag
+// before it reads its b, and writes x to the host array as rows finish.  The
+// side stream never waits on the kernel; the kernel's waits are bounded.
+int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cudaStream_t s)
+{
+    const int n = p->n;
+    const int nseg = (n + kStreamSegRows - 1) / kStreamSegRows;
+    if (!p->bflag || p->nseg < nseg) {
+        cudaFree(p->bflag);
+        p->bflag = nullptr;
+        SPT_CUDA(dalloc(&p->bflag, nseg));
+        SPT_CUDA(cudaMemset(p->bflag, 0, sizeof(int) * (size_t)nseg));
+        p->nseg = nseg;
+    }
+    if (!p->epochs) {
+        SPT_CUDA(cudaHostAlloc((void**)&p->epochs, sizeof(int) * 256, cudaHostAllocDefault));
+        for (int e = 0; e < 256; e++) p->epochs[e] = e;
+    }
+    if (!p->copy_stream) SPT_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    if (!p->ev_start) SPT_CUDA(cudaEventCreateWithFlags(&p->ev_start, cudaEventDisableTiming));
+    if (!p->ev_copied) SPT_CUDA(cudaEventCreateWithFlags(&p->ev_copied, cudaEventDisableTiming));
+    p->epoch = p->epoch % 255 + 1;  // 1..255: never the flags' initial 0, never the previous call's value
+    // the copies overwrite the device b only after everything queued before
+    // this call on s; the kernel is queued first (its waits cover the copies),
+    // so the time the host spends queueing the copies overlaps the solve
+    SPT_CUDA(cudaEventRecord(p->ev_start, s));
+    SPT_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_start, 0));
+    p->launch_bflag = p->bflag;
+    p->launch_epoch = p->epoch;
+    p->launch_hx = hx_dev;
+    int e = plan_solve_f64(p, p->hb, p->hx, 1, s);
+    p->launch_bflag = nullptr;
+    p->launch_hx = nullptr;
+    if (e) return e;
+    for (int g = 0; g < nseg; g++) {
+        const size_t r0 = (size_t)g * kStreamSegRows, rows = std::min<size_t>(kStreamSegRows, n - r0);
+        SPT_CUDA(cudaMemcpyAsync(p->hb + r0, hb + r0, sizeof(double) * rows, cudaMemcpyHostToDevice,
+                                 p->copy_stream));
+        SPT_CUDA(cudaMemcpyAsync(p->bflag + g, p->epochs + p->epoch, sizeof(int), cudaMemcpyHostToDevice,
+                                 p->copy_stream));
+    }
+    SPT_CUDA(cudaEventRecord(p->ev_copied, p->copy_stream));
+    SPT_CUDA(cudaStreamWaitEvent(s, p->ev_copied, 0));  // s's later work also comes after the copies
+    return 0;
 }
 
 sptrsv_schedule_t default_schedule()
@@ -298,7 +371,8 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         const size_t smem = (size_t)t.cap * sizeof(T);
         SPT_CUDA(allow_smem(kern, smem));
         SPT_CUDA(launch_persistent_capped(kern, block, smem, t.ngroups, cap, s, m, t.ngroups, b, x, x64, c->d_status,
-                                          budget, backoff));
+                                          budget, backoff, p->launch_bflag, kStreamSegRows, p->launch_epoch,
+                                          p->launch_hx));
         return 0;
     }
     const V *val, *dg, *di;
@@ -698,6 +772,15 @@ int sptrsv_solve_host(sptrsv_plan_t p, const double* hb, double* hx, int nrhs, i
         SPT_CUDA(cudaMalloc((void**)&p->hb, bytes));
         SPT_CUDA(cudaMalloc((void**)&p->hx, bytes));
         p->cap_host = nrhs;
+    }
+    void* hx_dev = nullptr;
+    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && mapped_host(hb) &&
+        (hx_dev = mapped_host(hx)) != nullptr) {
+        int e = build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
+        if (!e) e = solve_host_streamed(p, hb, (double*)hx_dev, s);
+        if (e) return e;
+        e = sync_status(s);
+        return e ? e : ok();
     }
     SPT_CUDA(cudaMemcpyAsync(p->hb, hb, bytes, cudaMemcpyHostToDevice, s));
     int e = precision == 32 ? plan_solve_ir(p, p->hb, p->hx, nrhs, s) : plan_solve_f64(p, p->hb, p->hx, nrhs, s);

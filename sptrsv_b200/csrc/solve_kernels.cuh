@@ -391,9 +391,9 @@ __device__ __forceinline__ void strip_meta(StripMeta<T>& z, const StripMat<V>& m
 
 template <typename V, typename T, typename BT>
 __device__ __forceinline__ void strip_ent(StripEnt<T>& z, const StripMeta<T>& md, const StripMat<V>& m,
-                                          const BT* __restrict__ b)
+                                          const BT* __restrict__ b, bool coherent_b = false)
 {
-    z.b = md.row >= 0 ? (T)b[md.row] : (T)0;
+    z.b = md.row >= 0 ? (T)(coherent_b ? ld_relaxed(b + md.row) : b[md.row]) : (T)0;
 #pragma unroll
     for (int u = 0; u < kStripU; u++) {
         z.cc[u] = 0;
@@ -485,6 +485,13 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstr
 // on the previous group, far planes) are polled in x.  After a group every
 // warp meets at a CTA barrier before the shared copy is reused; a warp
 // whose wait ran out raises a CTA flag there and the CTA leaves.
+//
+// Streamed host solves (bflag != nullptr): b arrives in segments of
+// seg_rows rows while the kernel runs, each segment followed by its flag
+// word set to `epoch`; a warp waits (acquire) for the flag of a row's
+// segment before it loads that row's b (only when the row's segment differs
+// from the last one the lane confirmed), and reads b coherently.  With hx
+// set, every x value is also written to that (mapped, pinned) host array.
 template <typename V>
 struct WaveMat {
     StripMat<V> c;                 // slot arrays (sptr unused)
@@ -496,7 +503,8 @@ struct WaveMat {
 template <typename V, typename T, typename BT, int OUT>
 __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroups, const BT* __restrict__ b, T* x,
                                                         double* x64, DevStatus* st, unsigned long long budget,
-                                                        unsigned backoff)
+                                                        unsigned backoff, const int* bflag, int seg_rows, int epoch,
+                                                        double* hx)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_flag;
@@ -505,6 +513,15 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const StripMat<V>& m = w.c;
     if (threadIdx.x == 0) abort_flag = 0;
+    int seg_ok = -1;  // streamed b: the last segment whose flag this lane saw set
+    auto b_ready = [&](int row) -> bool {
+        const int sg = row >= 0 ? row / seg_rows : seg_ok;
+        const bool need = bflag != nullptr && sg != seg_ok;
+        if (!__any_sync(FULL, need)) return true;
+        if (!warp_wait_flag(need, bflag + (need ? sg : 0), epoch, st, budget, row)) return false;
+        if (need) seg_ok = sg;
+        return true;
+    };
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const int r0 = __ldg(w.grow + g), nr = __ldg(w.grow + g + 1) - r0;
         for (int t = threadIdx.x; t < nr; t += blockDim.x) xs[t] = sentinel_value<T>();
@@ -516,14 +533,19 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
             StripMeta<T> m0, m1;
             StripEnt<T> e0;
             strip_meta<V, T>(m0, m, q0 * 32 + lane);
-            strip_ent<V, T, BT>(e0, m0, m, b);
+            if (!b_ready(m0.row)) failed = true;
+            strip_ent<V, T, BT>(e0, m0, m, b, bflag != nullptr);
             if (q0 + 1 < q1) strip_meta<V, T>(m1, m, (q0 + 1) * 32 + lane);
             for (int q = q0; q < q1 && !failed; q++) {
                 const StripMeta<T> md = m0;
                 const StripEnt<T> en = e0;
                 if (q + 1 < q1) {
                     m0 = m1;
-                    strip_ent<V, T, BT>(e0, m0, m, b);
+                    if (!b_ready(m0.row)) {
+                        failed = true;
+                        break;
+                    }
+                    strip_ent<V, T, BT>(e0, m0, m, b, bflag != nullptr);
                     if (q + 2 < q1) strip_meta<V, T>(m1, m, (q + 2) * 32 + lane);
                 }
                 const int ec = md.e1 - md.e0;
@@ -568,6 +590,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                 if (md.row >= 0) {
                     xs[md.row - r0] = xi;
                     publish<T, OUT>(x, x64, md.row, xi);
+                    if (hx) hx[md.row] = (double)xi;
                 }
             }
         }

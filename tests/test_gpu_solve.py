@@ -396,3 +396,38 @@ def test_strip_full_size_grid(torch_cuda):
         assert O.rel_err(dx.cpu().numpy(), ref) <= TOL, sc
     plan.close()
     S.free_device_analysis(L, info)
+
+
+@pytest.mark.parametrize("shape", [(512, 600), (100, 77)], ids=["three_segments", "small"])
+def test_streamed_host_solve(torch_cuda, shape):
+    """Host-buffer solves of a WAVE plan with pinned b and x copy b in
+    segments while the solve runs and write x to the host as rows finish: the
+    result matches the oracle call after call (the segment flags' epochs wrap
+    after 255 calls, and b changes between calls), and pageable buffers take
+    the plain copy path."""
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.grid2d(*shape, seed=3)
+    xt = gen.vector(m.n, "uniform", seed=4)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    plan.set_schedule(variant=S._lib.VAR_WAVE, block_warps=4)
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.empty(m.n, dtype=torch.float64).pin_memory()
+    reps = 260 if m.n < 100_000 else 6
+    for r in range(reps):
+        scale = 1.0 + r % 3
+        hb.copy_(torch.from_numpy(b * scale))
+        hx.fill_(float("nan"))
+        plan.solve_host(hb, hx, 1, 64)
+        assert O.rel_err(hx.numpy(), ref * scale) <= TOL, r
+    xp = np.zeros(m.n)
+    plan.solve_host(b, xp, 1, 64)
+    assert O.rel_err(xp, ref) <= TOL
+    plan.solve_host(hb, hx, 1, 32)  # FP32 + refinement: the plain copy path
+    assert O.rel_err(hx.numpy(), ref * (1.0 + (reps - 1) % 3)) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
