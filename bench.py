@@ -596,8 +596,8 @@ def run_batch(args, rank, world, local, dist):
 
     # --- schedule: level-ordered vs hybrid, block size, refinement steps (exhaustive, small)
     cands = []
-    for mode, width in ((0, 0.0), (2, 16.0)):
-        for bw in (8, 16):
+    for mode, width in ((0, 0.0), (2, 16.0), (2, 32.0)):
+        for bw in (2, 4, 8):
             cands.append((mode, width, bw))
     res = {}
     for mode, width, bw in cands:

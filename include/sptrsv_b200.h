@@ -316,8 +316,10 @@ int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int mode, int block_warps, i
                               int backoff_ns, int ir_iters);
 /* Width threshold of mode 2 (default 16): a system is sequential when
  * n_s / nlevs_s < width and all its dependencies reach back at most
- * 1024 / kp rows (kp = power of two >= its right-hand-side count); 0 makes
- * no system sequential, >= 1e9 makes every system sequential. */
+ * 1024 / kp rows (kp = power of two >= its right-hand-side count), or 1024
+ * rows for a system with more than 8 right-hand sides or of at least 16384
+ * rows with several (solved one right-hand side per warp); 0 makes no system
+ * sequential, >= 1e9 makes every system sequential. */
 int sptrsv_batch_set_seq_width(sptrsv_batch_t batch, double width);
 /* Systems solved sequentially, warps they occupy, rows left to the level tasks. */
 int sptrsv_batch_seq_systems(sptrsv_batch_t batch, int* nseq, int* nseq_warps, int* n_level_rows);

@@ -32,6 +32,7 @@
 //   tbase[ntasks+1], tkp[ntasks].
 #include <algorithm>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -89,7 +90,8 @@ struct sptrsv_batch_s {
     std::vector<char> seq;       // [nsys] 1: solved by one warp in natural order (mode 2)
     int n_lvl = 0;               // rows in the level layout (the non-sequential systems)
     int* wptr = nullptr;         // [nseqw+1] per sequential warp: range in wsys
-    int* wsys = nullptr;         // systems in sequential-warp order
+    int* wsys = nullptr;         // units in sequential-warp order: system
+    int* wcol = nullptr;         // and right-hand side (-1: all of them)
     int nseqw = 0;
     double seq_width = 16.0;     // mode 2: sequential when n_s / nlevs_s < seq_width
     int mode = 2;                // 0: level-ordered tasks, 1: natural-order chunks, 2: hybrid
@@ -122,13 +124,15 @@ struct SeqSet {
     const int* __restrict__ sk;      // [nsys]
     const long long* __restrict__ soff;
     const int* __restrict__ wptr;    // [nseqw+1]
-    const int* __restrict__ wsys;
+    const int* __restrict__ wsys;    // per unit: system
+    const int* __restrict__ wcol;    // per unit: right-hand side (-1: all of them)
     int nseqw;
 };
 
 constexpr int kVkU = 8;         // elements per wait round in the level-ordered kernel
 constexpr int kSeqRing = 1024;  // ring elements per sequential warp
 constexpr int kSeqEC = 512;     // entries of one 32-row chunk that fit a stage buffer
+constexpr int kSeqMaxK = 8;     // most right-hand sides one sequential warp carries (more: one warp per column)
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes_is8)
 {
@@ -148,30 +152,35 @@ struct SeqSmem {
     static constexpr size_t ring = al(kSeqRing * sizeof(T));
     static constexpr size_t o_ptr = 0, o_di = al(33 * 4), o_col = o_di + al(32 * sizeof(V)),
                             o_val = o_col + al(kSeqEC * 4), o_b = o_val + al(kSeqEC * sizeof(V)),
-                            buf = o_b + al(32 * 32 * sizeof(BT));
+                            buf = o_b + al(32 * kSeqMaxK * sizeof(BT));
     static constexpr size_t total = ring + 2 * buf;
 };
 
-// One warp solves system s in natural order without waiting on anyone.
+// One warp solves system s (right-hand side col only, or all of them when
+// col < 0) in natural order without waiting on anyone.
 // Chunks of 32 rows are staged into shared memory with cp.async one chunk
 // ahead (their row pointers are loaded two chunks ahead), so a row's work
 // reads only shared memory: its entries, its right-hand sides and, for
 // columns at most rw rows back, the ring of recent x values (slot = row mod
 // rw).  An older column is read back from x, which this warp wrote.  Lane q
-// owns right-hand side q (K > 1, products subtracted in element order), or
-// the lanes stride a row's entries and reduce (K == 1).  A chunk with more
-// than kSeqEC entries is read from global memory instead.
+// owns right-hand side q (all of K > 1 columns, products subtracted in
+// element order), or, for one column, lane j owns row j of each chunk (a
+// sweep; the column's values are strided by K in b and x).  A chunk with
+// more than kSeqEC entries is read from global memory instead.
 template <typename V, typename T, typename BT, int OUT>
 __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict__ val, const V* __restrict__ di,
-                                           int s, const BT* __restrict__ b, T* x, double* x64, unsigned char* region)
+                                           int s, int col, const BT* __restrict__ b, T* x, double* x64,
+                                           unsigned char* region)
 {
     using SM = SeqSmem<V, T, BT>;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int r0 = __ldg(q.row0 + s), r1 = __ldg(q.row0 + s + 1), K = __ldg(q.sk + s);
     const long long off = __ldg(q.soff + s);
+    const int Ke = col >= 0 ? 1 : K;   // columns this warp carries
+    const int c0 = col >= 0 ? col : 0; // first of them
     int kp = 1;
-    while (kp < K) kp <<= 1;
+    while (kp < Ke) kp <<= 1;
     const int rw = kSeqRing / kp;
     const bool lk = lane < K;
     T* ring = reinterpret_cast<T*>(region);
@@ -204,7 +213,10 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                 cp_async(sval + p, val + a + p, sizeof(V) == 8);
             }
         const long long bo = off + (long long)(cb - r0) * K;
-        for (int p = lane; p < cnt * K; p += 32) cp_async(sb + p, b + bo + p, sizeof(BT) == 8);
+        if (Ke == 1)
+            for (int p = lane; p < cnt; p += 32) cp_async(sb + p, b + bo + (long long)p * K + c0, sizeof(BT) == 8);
+        else
+            for (int p = lane; p < cnt * K; p += 32) cp_async(sb + p, b + bo + p, sizeof(BT) == 8);
         cp_async_commit();
         a_out = a;
         return fits;
@@ -231,7 +243,7 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
         const BT* __restrict__ sb = reinterpret_cast<const BT*>(base + SM::o_b);
         const int* gcol = q.col + a_cur;
         const V* gval = val + a_cur;
-        if (K == 1) {
+        if (Ke == 1) {
             // lane j owns row cb + j: first the entries before the chunk
             // (final values, a sorted prefix of the row), then a sweep over
             // the chunk in which row t's value is broadcast and every later
@@ -252,7 +264,7 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                     nv = vv;
                     break;
                 }
-                acc -= vv * ((i - cc <= rw) ? ring[cc & (rw - 1)] : __ldcg(x + off + (cc - r0)));
+                acc -= vv * ((i - cc <= rw) ? ring[cc & (rw - 1)] : __ldcg(x + off + (long long)(cc - r0) * K + c0));
             }
             T res = 0;
             for (int t = 0; t < cnt; t++) {
@@ -270,7 +282,7 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
             }
             if (own) {
                 ring[i & (rw - 1)] = res;
-                const long long xi = off + (i - r0);
+                const long long xi = off + (long long)(i - r0) * K + c0;
                 x[xi] = res;
                 if (OUT == 1) x64[xi] = (double)res;
                 if (OUT == 2) x64[xi] += (double)res;
@@ -357,9 +369,10 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_vk(BatchMat bm, const V* __re
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int w = wib * (int)gridDim.x + (int)blockIdx.x;
-    if (w < q.nseqw) {  // w < nseqw implies wib == 0: one sequential warp per block
+    if (w < q.nseqw) {  // w < nseqw implies wib < the sequential warps per block, each with its region
         for (int z = __ldg(q.wptr + w); z < __ldg(q.wptr + w + 1); z++)
-            seq_system<V, T, BT, OUT>(q, nval, ndi, __ldg(q.wsys + z), b, x, x64, smem_raw);
+            seq_system<V, T, BT, OUT>(q, nval, ndi, __ldg(q.wsys + z), __ldg(q.wcol + z), b, x, x64,
+                                      smem_raw + (size_t)wib * SeqSmem<V, T, BT>::total);
         return;
     }
     const int gw = w - q.nseqw;
@@ -710,6 +723,7 @@ void batch_free(sptrsv_batch_s* B)
     cudaFree(B->ndi64); cudaFree(B->ndi32); cudaFree(B->tsys); cudaFree(B->tj); cudaFree(B->cdep);
     cudaFree(B->sys_row0); cudaFree(B->sys_chunk0); cudaFree(B->sys_k); cudaFree(B->sys_off); cudaFree(B->flags);
     cudaFree(B->row_sys); cudaFree(B->lev); cudaFree(B->d_kplog); cudaFree(B->wptr); cudaFree(B->wsys);
+    cudaFree(B->wcol);
     cudaFree(B->sys_task0);
     cudaFree(B->ptr); cudaFree(B->xrow); cudaFree(B->krow); cudaFree(B->xdep); cudaFree(B->val64);
     cudaFree(B->val32); cudaFree(B->dg64); cudaFree(B->di64); cudaFree(B->di32); cudaFree(B->tbase);
@@ -813,6 +827,11 @@ int batch_level_layout(sptrsv_batch_s* B, cudaStream_t s)
 
 constexpr int kModeLevel = 0, kModeChunk = 1, kModeHybrid = 2;
 constexpr double kSeqAll = 1e9;  // a sequential width this large makes every system sequential
+constexpr int kSeqSplitRows = 16384;  // sequential systems this long get one warp per right-hand side
+
+// Sequential warps per block (warps 0.. of each block), each with its own
+// shared-memory region; the other warps take the level tasks.
+int seq_per_block(const sptrsv_batch_s* B) { return B->block_warps >= 8 ? 4 : B->block_warps >= 4 ? 2 : 1; }
 
 
 // The level-ordered launch's grid size (every instantiation that a solve
@@ -821,22 +840,28 @@ template <typename V, typename T, typename BT, int OUT>
 int vk_grid(const sptrsv_batch_s* B, long long max_blocks, long long* g)
 {
     const int cap = B->warps_per_sm > 0 ? (B->warps_per_sm + B->block_warps - 1) / B->block_warps : 0;
-    const size_t smem = SeqSmem<V, T, BT>::total;
-    SPT_CUDA(persistent_grid(k_sptrsv_vk<V, T, BT, OUT>, 32 * B->block_warps, smem, max_blocks, cap, g));
+    const size_t smem = (size_t)seq_per_block(B) * SeqSmem<V, T, BT>::total;
+    auto kern = k_sptrsv_vk<V, T, BT, OUT>;
+    if (smem > 48 * 1024)  // the occupancy query needs the kernel's opt-in to large shared memory
+        SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SPT_CUDA(persistent_grid(kern, 32 * B->block_warps, smem, max_blocks, cap, g));
     return 0;
 }
 
 long long vk_max_blocks(const sptrsv_batch_s* B, int nseqw)
 {
-    const long long a = div_up(B->ntasks, B->block_warps), c = nseqw;
+    const long long a = div_up(B->ntasks, B->block_warps), c = div_up(nseqw, seq_per_block(B));
     return std::max(std::max(a, c), 1LL);
 }
 
 // Marks the sequential systems (mode 2: n_s / nlevs_s < seq_width and every
-// dependency within the ring window of the system's right-hand-side class,
-// or every system when seq_width >= kSeqAll), rebuilds the level layout when
+// dependency within the ring window: kSeqRing / kp rows, or kSeqRing rows for
+// a system with more than kSeqMaxK right-hand sides or of at least
+// kSeqSplitRows rows and several right-hand sides, which is solved one column
+// per warp; or every system when seq_width >= kSeqAll),
+// rebuilds the level layout when
 // the set changed, and spreads the sequential systems
-// over at most one warp per block of the grid, largest first, each to the warp
+// over at most seq_per_block warps per block of the grid, largest first, each to the warp
 // with the least work so far.
 int batch_apply_schedule(sptrsv_batch_s* B, cudaStream_t s)
 {
@@ -846,7 +871,9 @@ int batch_apply_schedule(sptrsv_batch_s* B, cudaStream_t s)
             const double nk = B->row0h[k + 1] - B->row0h[k];
             int kp = 1;
             while (kp < B->kk[k]) kp <<= 1;
-            const bool fits = B->sys_dist[k] <= kSeqRing / kp;
+            // a split system's units carry one column each: their ring spans kSeqRing rows
+            const bool split = B->kk[k] > kSeqMaxK || (B->kk[k] > 1 && nk >= kSeqSplitRows);
+            const bool fits = B->sys_dist[k] <= (split ? kSeqRing : kSeqRing / kp);
             seq[k] = B->seq_width >= kSeqAll || (fits && nk < B->seq_width * std::max(1, B->sys_nlev[k]));
         }
     if (seq != B->seq || !B->ptr) {
@@ -854,12 +881,23 @@ int batch_apply_schedule(sptrsv_batch_s* B, cudaStream_t s)
         int e = batch_level_layout(B, s);
         if (e) return e;
     }
-    std::vector<int> list;
-    for (int k = 0; k < B->nsys; k++)
-        if (B->seq[k]) list.push_back(k);
+    // units: a system with more than kSeqMaxK right-hand sides, or a long one
+    // with several, becomes one unit per column (each swept by its own warp,
+    // 0.13 us per row on a near-chain); other systems are one unit carrying
+    // all their columns (0.4 us per row for K > 1)
+    std::vector<std::pair<int, int>> list;
+    for (int k = 0; k < B->nsys; k++) {
+        if (!B->seq[k]) continue;
+        const int nk = B->row0h[k + 1] - B->row0h[k];
+        if (B->kk[k] > kSeqMaxK || (B->kk[k] > 1 && nk >= kSeqSplitRows))
+            for (int c = 0; c < B->kk[k]; c++) list.push_back({k, c});
+        else
+            list.push_back({k, -1});
+    }
     cudaFree(B->wptr);
     cudaFree(B->wsys);
-    B->wptr = B->wsys = nullptr;
+    cudaFree(B->wcol);
+    B->wptr = B->wsys = B->wcol = nullptr;
     B->nseqw = 0;
     if (list.empty()) return 0;
     long long g = 0, gmin = 1LL << 40;
@@ -871,25 +909,35 @@ int batch_apply_schedule(sptrsv_batch_s* B, cudaStream_t s)
     gmin = std::min(gmin, g);
     if ((e = vk_grid<float, float, float, 2>(B, mb, &g))) return e;
     gmin = std::min(gmin, g);
-    const int nw = (int)std::min<long long>((long long)list.size(), gmin);
-    auto work = [&](int k) { return (double)(B->row0h[k + 1] - B->row0h[k]) * (1.0 + B->kk[k] / 8.0); };
-    std::stable_sort(list.begin(), list.end(), [&](int a, int b2) { return work(a) > work(b2); });
-    std::vector<std::vector<int>> per(nw);
+    const int nw = (int)std::min<long long>((long long)list.size(), gmin * seq_per_block(B));
+    auto work = [&](const std::pair<int, int>& u) {
+        const double nk = B->row0h[u.first + 1] - B->row0h[u.first];
+        return nk * (u.second >= 0 || B->kk[u.first] == 1 ? 1.0 : 3.0);
+    };
+    std::stable_sort(list.begin(), list.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b2) {
+        return work(a) > work(b2);
+    });
+    std::vector<std::vector<std::pair<int, int>>> per(nw);
     std::vector<double> load(nw, 0.0);
-    for (int k : list) {
+    for (const auto& u : list) {
         const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        per[w].push_back(k);
-        load[w] += work(k);
+        per[w].push_back(u);
+        load[w] += work(u);
     }
-    std::vector<int> wp(nw + 1, 0), ws;
+    std::vector<int> wp(nw + 1, 0), ws, wc;
     for (int w = 0; w < nw; w++) {
-        ws.insert(ws.end(), per[w].begin(), per[w].end());
+        for (const auto& u : per[w]) {
+            ws.push_back(u.first);
+            wc.push_back(u.second);
+        }
         wp[w + 1] = (int)ws.size();
     }
     SPT_CUDA(dalloc(&B->wptr, nw + 1));
     SPT_CUDA(dalloc(&B->wsys, (long long)ws.size()));
+    SPT_CUDA(dalloc(&B->wcol, (long long)wc.size()));
     SPT_CUDA(cudaMemcpy(B->wptr, wp.data(), sizeof(int) * wp.size(), cudaMemcpyHostToDevice));
     SPT_CUDA(cudaMemcpy(B->wsys, ws.data(), sizeof(int) * ws.size(), cudaMemcpyHostToDevice));
+    SPT_CUDA(cudaMemcpy(B->wcol, wc.data(), sizeof(int) * wc.size(), cudaMemcpyHostToDevice));
     B->nseqw = nw;
     return 0;
 }
@@ -919,9 +967,9 @@ int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cu
     const V* nval = f32 ? reinterpret_cast<const V*>(B->nval32) : reinterpret_cast<const V*>(B->nval64);
     const V* ndi = f32 ? reinterpret_cast<const V*>(B->ndi32) : reinterpret_cast<const V*>(B->ndi64);
     BatchMat bm{B->ptr, B->xrow, B->krow, B->xdep};
-    SeqSet q{B->nptr, B->ncol, B->sys_row0, B->sys_k, B->sys_off, B->wptr, B->wsys, B->nseqw};
+    SeqSet q{B->nptr, B->ncol, B->sys_row0, B->sys_k, B->sys_off, B->wptr, B->wsys, B->wcol, B->nseqw};
     auto kern = k_sptrsv_vk<V, T, BT, OUT>;
-    const size_t smem = B->nseqw > 0 ? SeqSmem<V, T, BT>::total : 0;
+    const size_t smem = B->nseqw > 0 ? (size_t)seq_per_block(B) * SeqSmem<V, T, BT>::total : 0;
     if (smem > 48 * 1024)
         SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (B->ntasks == 0 && B->nseqw == 0) return 0;
@@ -1013,11 +1061,12 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
         cudaFree(d_sys); cudaFree(d_row0); cudaFree(d_kplog); cudaFree(d_sk); cudaFree(d_soff);
     };
     auto fail = [&](int code) {
+        std::string msg = sptrsv_last_error_string();  // the public free below resets the last error
         cleanup();
         free_device_analysis(nullptr, &info);
         batch_free(B);
         delete B;
-        return code;
+        return set_error(code, "%s", msg.c_str());
     };
 #define BCHK(call)                                                 \
     do {                                                           \

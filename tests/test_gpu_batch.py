@@ -138,3 +138,35 @@ def test_batch_hybrid_many_systems_per_warp(torch_cuda, precision):
     batch.close()
     for d in dev:
         S.free_device_analysis(d, None)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_long_chains_one_warp_per_rhs(torch_cuda, precision):
+    """Long near-chain systems with several right-hand sides are solved by one
+    warp per right-hand side (strided columns of b and x): more sequential
+    warps than systems, results as the oracle's."""
+    import sptrsv_b200 as S
+    from sptrsv_b200.batch import Batch
+
+    torch = torch_cuda
+    mats, ks, xs = gen.batch_config(6, seed=13, n_lo=20000, n_hi=40000, bw_lo=8, bw_hi=20, k_max=9)
+    dev = [S.allocate_memory(m.rowptr, m.colidx, m.val, m.n) for m in mats]
+    bs = [m.matvec(x, k) for m, x, k in zip(mats, xs, ks)]
+    refs = [O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k) for m, b, k in zip(mats, bs, ks)]
+    batch = Batch(dev, ks)
+    batch.set_seq_width(16.0)
+    batch.set_schedule(mode=2, block_warps=8, ir_iters=2)
+    nseq, nw, _ = batch.seq_systems()
+    assert nseq == len(mats) and nw > nseq, (nseq, nw, ks)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.empty_like(db)
+    for rep in range(2):
+        batch.solve(db, dx, precision)
+        S.sync_status()
+        xh = dx.cpu().numpy()
+        for s in range(len(mats)):
+            a, b = batch.offsets[s], batch.offsets[s + 1]
+            assert O.rel_err(xh[a:b], refs[s]) <= TOL, (rep, s)
+    batch.close()
+    for d in dev:
+        S.free_device_analysis(d, None)
