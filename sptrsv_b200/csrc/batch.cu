@@ -82,8 +82,9 @@ struct sptrsv_batch_s {
     // per-system level structure and the hybrid schedule
     int* lev = nullptr;          // [n] level of each union row (1-based)
     int* d_kplog = nullptr;      // [nsys] log2 of the right-hand-side class
-    int* sys_task0 = nullptr;    // [nsys+1] first residual task of each system (32/kp rows per task)
-    int nres_tasks = 0;
+    int* rblk_sys = nullptr;     // residual blocks: system of each 256-element block
+    int* rblk_e0 = nullptr;      // and its first element inside the system
+    int nrblk = 0;
     std::vector<int> row0h;      // [nsys+1] first union row of each system
     std::vector<int> sys_nlev;   // [nsys] levels of each system
     std::vector<int> sys_dist;   // [nsys] largest row - column distance of an entry
@@ -251,6 +252,8 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
             const int j = lane, i = cb + j;
             const bool own = j < cnt;
             T acc = own ? (T)sb[j] : (T)0;
+            // the accumulated solution this correction adds to, loaded before the sweep
+            const double old64 = (OUT == 2 && own) ? x64[off + (long long)(i - r0) * K + c0] : 0.0;
             const T piv = own ? (T)sdi[j] : (T)0;
             int p = own ? sptr[j] : 0;
             const int pe = own ? sptr[j + 1] : 0;
@@ -285,7 +288,7 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                 const long long xi = off + (long long)(i - r0) * K + c0;
                 x[xi] = res;
                 if (OUT == 1) x64[xi] = (double)res;
-                if (OUT == 2) x64[xi] += (double)res;
+                if (OUT == 2) x64[xi] = old64 + (double)res;
             }
         } else {
             // lane q owns right-hand side q; rows one after another.  A row's
@@ -297,14 +300,18 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                 T* __restrict__ rl = ring + lane;
                 int e0 = sptr[0], e1 = sptr[1];
                 T piv = (T)sdi[0], bj = (T)sb[lane];
+                const long long xb = off + (long long)(cb - r0) * K + lane;  // x index of the chunk's first row
+                double old64 = OUT == 2 ? x64[xb] : 0.0;  // the solution a correction adds to, a row ahead
                 for (int j = 0; j < cnt; j++) {
                     const int i = cb + j;
                     int ne1 = 0;
                     T npiv = 0, nbj = 0;
+                    double nold64 = 0.0;
                     if (j + 1 < cnt) {
                         ne1 = sptr[j + 2];
                         npiv = (T)sdi[j + 1];
                         nbj = (T)sb[(j + 1) * K + lane];
+                        if (OUT == 2) nold64 = x64[xb + (long long)(j + 1) * K];
                     }
                     T acc = bj;
                     int p = e0;
@@ -339,11 +346,12 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                     const long long xi = off + (long long)(i - r0) * K + lane;
                     x[xi] = res;
                     if (OUT == 1) x64[xi] = (double)res;
-                    if (OUT == 2) x64[xi] += (double)res;
+                    if (OUT == 2) x64[xi] = old64 + (double)res;
                     e0 = e1;
                     e1 = ne1;
                     piv = npiv;
                     bj = nbj;
+                    old64 = nold64;
                 }
             }
         }
@@ -385,9 +393,11 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_vk(BatchMat bm, const V* __re
         long long xr = 0;
         T acc = 0, piv = 0;
         int s = 0, len = 0;
+        double old64 = 0.0;  // the solution a correction adds to, loaded with the task
         if (act) {
             xr = __ldg(bm.xrow + pos);
             acc = (T)b[xr + k];
+            if (OUT == 2) old64 = x64[xr + k];
             piv = (T)__ldg(di + pos);
             s = __ldg(bm.ptr + pos);
             len = __ldg(bm.ptr + pos + 1) - s;
@@ -417,7 +427,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_vk(BatchMat bm, const V* __re
             T r = publishable(acc * piv);
             st_relaxed(x + xr + k, r);
             if (OUT == 1) x64[xr + k] = (double)r;
-            if (OUT == 2) x64[xr + k] += (double)r;
+            if (OUT == 2) x64[xr + k] = old64 + (double)r;
         }
     }
 }
@@ -502,50 +512,43 @@ __global__ void __launch_bounds__(256) k_sptrsv_vkc(NatBatch nb, const V* __rest
     }
 }
 
-// r = b - L x in FP64 over the natural-order union (no dependencies).  Warp
-// task t covers 32/kp consecutive rows of one system (kp lanes per row, lane
-// k of a row owns right-hand side k); sys_task0[s] is the first task of
-// system s.  Elements are taken four at a time so their loads overlap.
+// r = b - L x in FP64 over the natural-order union (no dependencies), one
+// thread per element of the packed vectors: block t covers the 256
+// elements of system rblk_sys[t] starting at its element rblk_e0[t]
+// (blocks never cross systems), element e of a system with K right-hand
+// sides is (row e / K, column e mod K).  Threads of one row share its
+// entries through L1; b, x and r are read and written coalesced.
 __global__ void __launch_bounds__(256) k_residual_nat(const int* __restrict__ ptr, const int* __restrict__ col,
                                                       const double* __restrict__ val, const double* __restrict__ dg,
-                                                      const int* __restrict__ sys_task0, int nsys,
+                                                      const int* __restrict__ rblk_sys, const int* __restrict__ rblk_e0,
                                                       const int* __restrict__ row0, const int* __restrict__ sk,
-                                                      const int* __restrict__ kplog,
                                                       const long long* __restrict__ soff, const double* __restrict__ b,
                                                       const double* __restrict__ x, float* __restrict__ r)
 {
-    const int lane = threadIdx.x & 31;
-    const int ntask = __ldg(sys_task0 + nsys);
-    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-    for (int t = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); t < ntask; t += nw) {
-        int lo = 0, hi = nsys - 1;  // system: largest s with sys_task0[s] <= t
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(sys_task0 + mid) <= t) lo = mid;
-            else hi = mid - 1;
-        }
-        const int s = lo, lg = __ldg(kplog + s), K = __ldg(sk + s), r0 = __ldg(row0 + s);
-        const int k = lane & ((1 << lg) - 1);
-        const int i = r0 + ((t - __ldg(sys_task0 + s)) << (5 - lg)) + (lane >> lg);
-        if (i >= __ldg(row0 + s + 1) || k >= K) continue;
-        const long long xb = soff[s] + k - (long long)r0 * K;  // x[xb + c * K]: row c, right-hand side k
-        const long long xr = xb + (long long)i * K;
-        double acc = b[xr] - dg[i] * x[xr];
-        int p = ptr[i];
-        const int e = ptr[i + 1];
-        for (; p + 4 <= e; p += 4) {
-            const int c0 = col[p], c1 = col[p + 1], c2 = col[p + 2], c3 = col[p + 3];
-            const double v0 = val[p], v1 = val[p + 1], v2 = val[p + 2], v3 = val[p + 3];
-            const double x0 = x[xb + (long long)c0 * K], x1 = x[xb + (long long)c1 * K],
-                         x2 = x[xb + (long long)c2 * K], x3 = x[xb + (long long)c3 * K];
-            acc -= v0 * x0;
-            acc -= v1 * x1;
-            acc -= v2 * x2;
-            acc -= v3 * x3;
-        }
-        for (; p < e; p++) acc -= val[p] * x[xb + (long long)col[p] * K];
-        r[xr] = (float)acc;
+    const int s = __ldg(rblk_sys + blockIdx.x);
+    const int r0 = __ldg(row0 + s), n_s = __ldg(row0 + s + 1) - r0, K = __ldg(sk + s);
+    const int e = __ldg(rblk_e0 + blockIdx.x) + threadIdx.x;
+    if (e >= n_s * K) return;
+    const int i = (int)(((double)e + 0.5) / (double)K);  // exact for e < 2^50
+    const int k = e - i * K;
+    const long long xb = __ldg(soff + s) + k - (long long)r0 * K;  // x[xb + c * K]: row c, right-hand side k
+    const long long xe = __ldg(soff + s) + e;
+    const int row = r0 + i;
+    double acc = b[xe] - __ldg(dg + row) * x[xe];
+    int p = __ldg(ptr + row);
+    const int pe = __ldg(ptr + row + 1);
+    for (; p + 4 <= pe; p += 4) {
+        const int c0 = __ldg(col + p), c1 = __ldg(col + p + 1), c2 = __ldg(col + p + 2), c3 = __ldg(col + p + 3);
+        const double v0 = __ldg(val + p), v1 = __ldg(val + p + 1), v2 = __ldg(val + p + 2), v3 = __ldg(val + p + 3);
+        const double x0 = x[xb + (long long)c0 * K], x1 = x[xb + (long long)c1 * K], x2 = x[xb + (long long)c2 * K],
+                     x3 = x[xb + (long long)c3 * K];
+        acc -= v0 * x0;
+        acc -= v1 * x1;
+        acc -= v2 * x2;
+        acc -= v3 * x3;
     }
+    for (; p < pe; p++) acc -= __ldg(val + p) * x[xb + (long long)__ldg(col + p) * K];
+    r[xe] = (float)acc;
 }
 
 // ---- build ----
@@ -724,7 +727,7 @@ void batch_free(sptrsv_batch_s* B)
     cudaFree(B->sys_row0); cudaFree(B->sys_chunk0); cudaFree(B->sys_k); cudaFree(B->sys_off); cudaFree(B->flags);
     cudaFree(B->row_sys); cudaFree(B->lev); cudaFree(B->d_kplog); cudaFree(B->wptr); cudaFree(B->wsys);
     cudaFree(B->wcol);
-    cudaFree(B->sys_task0);
+    cudaFree(B->rblk_sys); cudaFree(B->rblk_e0);
     cudaFree(B->ptr); cudaFree(B->xrow); cudaFree(B->krow); cudaFree(B->xdep); cudaFree(B->val64);
     cudaFree(B->val32); cudaFree(B->dg64); cudaFree(B->di64); cudaFree(B->di32); cudaFree(B->tbase);
     cudaFree(B->tkp); cudaFree(B->w32a); cudaFree(B->w32b);
@@ -981,9 +984,8 @@ int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cu
 
 int batch_residual(sptrsv_batch_s* B, const double* b, const double* x, cudaStream_t s)
 {
-    k_residual_nat<<<grid_for((long long)B->nres_tasks * 32, 256), 256, 0, s>>>(
-        B->nptr, B->ncol, B->nval64, B->ndg64, B->sys_task0, B->nsys, B->sys_row0, B->sys_k, B->d_kplog, B->sys_off, b,
-        x, B->w32b);
+    k_residual_nat<<<B->nrblk, 256, 0, s>>>(B->nptr, B->ncol, B->nval64, B->ndg64, B->rblk_sys, B->rblk_e0,
+                                             B->sys_row0, B->sys_k, B->sys_off, b, x, B->w32b);
     SPT_CUDA(cudaGetLastError());
     return 0;
 }
@@ -1126,18 +1128,20 @@ int sptrsv_batch_create(int nsys, const sp_mat_t* mats, const int* nrhs, sptrsv_
         BCHK(ce);
     }
     B->row0h = row0;
-    {  // residual tasks: 32/kp consecutive rows of one system each
-        std::vector<int> t0(nsys + 1, 0);
-        long long tot = 0;
+    {  // residual blocks: 256 consecutive packed elements of one system each
+        std::vector<int> bs, be;
         for (int k = 0; k < nsys; k++) {
-            t0[k] = (int)tot;
-            const int rows = 32 >> kplog[k];
-            tot += (mats[k].nr + rows - 1) / rows;
+            const long long ne = (long long)mats[k].nr * nrhs[k];
+            for (long long e0 = 0; e0 < ne; e0 += 256) {
+                bs.push_back(k);
+                be.push_back((int)e0);
+            }
         }
-        t0[nsys] = (int)tot;
-        B->nres_tasks = (int)tot;
-        BCHK(dalloc(&B->sys_task0, nsys + 1));
-        BCHK(cudaMemcpy(B->sys_task0, t0.data(), sizeof(int) * (size_t)(nsys + 1), cudaMemcpyHostToDevice));
+        B->nrblk = (int)bs.size();
+        BCHK(dalloc(&B->rblk_sys, B->nrblk));
+        BCHK(dalloc(&B->rblk_e0, B->nrblk));
+        BCHK(cudaMemcpy(B->rblk_sys, bs.data(), sizeof(int) * bs.size(), cudaMemcpyHostToDevice));
+        BCHK(cudaMemcpy(B->rblk_e0, be.data(), sizeof(int) * be.size(), cudaMemcpyHostToDevice));
     }
     // 5. natural-order chunk schedule: union without diagonals, chunk tasks in
     //    (chunk index, system) order, each with the first chunk it reads
