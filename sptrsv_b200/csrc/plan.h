@@ -68,6 +68,7 @@ struct WaveLayout {
     int* grun = nullptr;       // [ngroups+1] first run of each group
     int* grow = nullptr;       // [ngroups+1] first row of each group
     int ngroups = 0, G = 0, cap = 0;  // cap: most rows in one group
+    int maxe = 0;                      // most entries of one slot
 };
 
 struct sptrsv_plan_s {

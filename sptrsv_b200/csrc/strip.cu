@@ -111,6 +111,15 @@ __global__ void k_strip_slots(const int* __restrict__ chunk_at, const int* __res
     }
 }
 
+// *out = max(*out, a[0..n)) (non-negative values).
+__global__ void k_max_int(const int* __restrict__ a, int n, int* out)
+{
+    int m = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) m = max(m, a[t]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
 // Entries in processing order, encoded: ~slot for a column whose chunk this
 // warp solved fewer than W positions earlier in the same strip, else the
 // column.  flag |= 2 when a same-strip dependency does not come earlier.
@@ -475,6 +484,9 @@ int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows)
     WCHK(dalloc(&scr, scan_scratch_ints((long long)nslots + 1)));
     WCHK(dalloc(&w.pe, (long long)nslots + 1));
     WCHK(scan_exclusive(scnt, w.pe, (long long)nslots + 1, scr, s));
+    k_max_int<<<grid_for(nslots, 256), 256, 0, s>>>(scnt, nslots, scnt + nslots);  // scnt[nslots] was 0
+    WCHK(cudaGetLastError());
+    WCHK(cudaMemcpyAsync(&w.maxe, scnt + nslots, sizeof(int), cudaMemcpyDeviceToHost, s));
     WCHK(dalloc(&w.ecol, m));
     WCHK(dalloc(&w.ev64, m));
     WCHK(dalloc(&w.ev32, m));
