@@ -367,7 +367,13 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
                       f32 ? reinterpret_cast<const V*>(t.lsub32) : reinterpret_cast<const V*>(t.lsub64),
                       f32 ? reinterpret_cast<const V*>(t.di32) : reinterpret_cast<const V*>(t.di64), nullptr},
                      t.runc, t.grun, t.grow};
-        auto kern = t.maxe <= 2 ? k_sptrsv_wave<V, T, BT, OUT, 2> : k_sptrsv_wave<V, T, BT, OUT, kStripU>;
+        auto kern = p->launch_bflag
+                        ? (t.maxe <= 2         ? k_sptrsv_wave<V, T, BT, OUT, 2, false, true>
+                           : t.maxe <= kStripU ? k_sptrsv_wave<V, T, BT, OUT, kStripU, false, true>
+                                               : k_sptrsv_wave<V, T, BT, OUT, kStripU, true, true>)
+                        : (t.maxe <= 2         ? k_sptrsv_wave<V, T, BT, OUT, 2, false, false>
+                           : t.maxe <= kStripU ? k_sptrsv_wave<V, T, BT, OUT, kStripU, false, false>
+                                               : k_sptrsv_wave<V, T, BT, OUT, kStripU, true, false>);
         const size_t smem = (size_t)t.cap * sizeof(T);
         SPT_CUDA(allow_smem(kern, smem));
         SPT_CUDA(launch_persistent_capped(kern, block, smem, t.ngroups, cap, s, m, t.ngroups, b, x, x64, c->d_status,

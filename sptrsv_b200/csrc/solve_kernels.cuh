@@ -497,7 +497,8 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstr
 // row holds more than two entries outside its chunk recurrence (2D
 // stencils), which shortens the poll loop and the dependent arithmetic on
 // the line-to-line critical path (0.81 against 1.03 ms on a 2048 x 2048
-// grid), else U = kStripU.
+// grid), else U = kStripU.  MULTI: some row holds more than U such entries
+// (later rounds load theirs on the spot); STREAM: the streamed host solve.
 template <typename V>
 struct WaveMat {
     StripMat<V> c;                 // slot arrays (sptr unused)
@@ -506,7 +507,7 @@ struct WaveMat {
     const int* __restrict__ grow;  // first row of each group
 };
 
-template <typename V, typename T, typename BT, int OUT, int U>
+template <typename V, typename T, typename BT, int OUT, int U, bool MULTI, bool STREAM>
 __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroups, const BT* __restrict__ b, T* x,
                                                         double* x64, DevStatus* st, unsigned long long budget,
                                                         unsigned backoff, const int* bflag, int seg_rows, int epoch,
@@ -521,6 +522,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
     if (threadIdx.x == 0) abort_flag = 0;
     int seg_ok = -1;  // streamed b: the last segment whose flag this lane saw set
     auto b_ready = [&](int row) -> bool {
+        if (!STREAM) return true;
         const int sg = row >= 0 ? row / seg_rows : seg_ok;
         const bool need = bflag != nullptr && sg != seg_ok;
         if (!__any_sync(FULL, need)) return true;
@@ -540,7 +542,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
             StripEnt<T, U> e0;
             strip_meta<V, T>(m0, m, q0 * 32 + lane);
             if (!b_ready(m0.row)) failed = true;
-            strip_ent<V, T, BT, U>(e0, m0, m, b, bflag != nullptr);
+            strip_ent<V, T, BT, U>(e0, m0, m, b, STREAM);
             if (q0 + 1 < q1) strip_meta<V, T>(m1, m, (q0 + 1) * 32 + lane);
             for (int q = q0; q < q1 && !failed; q++) {
                 const StripMeta<T> md = m0;
@@ -551,12 +553,12 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                         failed = true;
                         break;
                     }
-                    strip_ent<V, T, BT, U>(e0, m0, m, b, bflag != nullptr);
+                    strip_ent<V, T, BT, U>(e0, m0, m, b, STREAM);
                     if (q + 2 < q1) strip_meta<V, T>(m1, m, (q + 2) * 32 + lane);
                 }
                 const int ec = md.e1 - md.e0;
                 T acc = en.b;
-                const int rounds = __reduce_max_sync(FULL, ec);
+                const int rounds = MULTI ? __reduce_max_sync(FULL, ec) : 1;
                 for (int j = 0; j < rounds; j += U) {
                     const int nh = min(U, ec - j);
                     int cc[U];
@@ -565,7 +567,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                     for (int u = 0; u < U; u++) {
                         cc[u] = en.cc[u];
                         vv[u] = en.vv[u];
-                        if (j > 0) {
+                        if (MULTI && j > 0) {
                             cc[u] = 0;
                             vv[u] = 0;
                             if (u < nh) {
@@ -596,7 +598,7 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                 if (md.row >= 0) {
                     xs[md.row - r0] = xi;
                     publish<T, OUT>(x, x64, md.row, xi);
-                    if (hx) hx[md.row] = (double)xi;
+                    if (STREAM && hx) hx[md.row] = (double)xi;
                 }
             }
         }

@@ -274,7 +274,34 @@ STRIP_OK = {
     "grid3d": lambda: gen.grid3d(40, 20, 15, seed=3),
     "grid3d_ragged": lambda: gen.grid3d(45, 13, 9, seed=4),
     "grid2d_short_lines": lambda: gen.grid2d(20, 90, seed=5),
+    "grid2d_long_lines": lambda: gen.grid2d(4000, 6, seed=6),
+    "uneven_lines": lambda: _uneven_lines(300, seed=7),
 }
+
+
+def _uneven_lines(nlines, seed):
+    """Lines of random lengths (1..150 rows): every row but a line's first
+    depends on the row before it, and most rows on the row at the same offset
+    of the line before when that line is long enough (the structure of a 2D
+    stencil on a ragged domain)."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(1, 151, size=nlines)
+    starts = np.concatenate([[0], np.cumsum(lens)])
+    rowptr, cols, vals = [0], [], []
+    for li in range(nlines):
+        for o in range(int(lens[li])):
+            i = int(starts[li]) + o
+            row = []
+            if li > 0 and o < lens[li - 1] and rng.random() < 0.9:
+                row.append(int(starts[li - 1]) + o)
+            if o > 0:
+                row.append(i - 1)
+            off = rng.uniform(-0.5, 0.5, size=len(row))
+            cols += row + [i]
+            vals += list(off) + [1.0 + float(np.abs(off).sum())]
+            rowptr.append(len(cols))
+    return gen.HostCsr(np.array(rowptr, dtype=np.int32), np.array(cols, dtype=np.int32),
+                       np.array(vals, dtype=np.float64))
 
 
 @pytest.mark.parametrize("name", list(STRIP_OK))
@@ -294,7 +321,9 @@ def test_strip_schedule_fp64_and_ir(torch_cuda, name):
     dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
     scheds = [dict(variant=S._lib.VAR_STRIP, rows_per_warp=r, block_warps=bw)
               for r, bw in ((1, 4), (2, 2), (4, 4), (8, 4), (16, 4), (32, 2))]
-    scheds += [dict(variant=S._lib.VAR_WAVE, block_warps=g) for g in (2, 4, 8, 16)]
+    # 4000-row lines: a group of more than 4 does not fit shared memory
+    gs = (2, 4) if name == "grid2d_long_lines" else (2, 4, 8, 16)
+    scheds += [dict(variant=S._lib.VAR_WAVE, block_warps=g) for g in gs]
     for sc in scheds:
         plan.set_schedule(ir_max_iters=2, **sc)
         for rep in range(2):
