@@ -375,7 +375,7 @@ def run_ours(args, rank, world, local, dist):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    m, xt, k = gen.config(args.config)
+    m, xt, k = gen.config(args.config, args.scale if args.lean else 1.0)
     b = m.matvec(xt, k)
     n, nnz = m.n, m.nnz
 
@@ -575,7 +575,7 @@ def run_batch(args, rank, world, local, dist):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    mats, ks, xs = gen.batch_config(512, seed=3)
+    mats, ks, xs = gen.batch_config(args.systems if args.lean else 512, seed=3)
     bs = [m.matvec(x, k) for m, x, k in zip(mats, xs, ks)]
     dev = [S.allocate_memory(m.rowptr, m.colidx, m.val, m.n) for m in mats]
     t0 = time.perf_counter()
@@ -588,6 +588,17 @@ def run_batch(args, rank, world, local, dist):
 
     def flush():
         flush_buf.fill_(1)
+
+    if args.lean:
+        # profiling run: the default hybrid schedule, warm-up and the timed solves, nothing else
+        prec = args.lean
+        batch.set_seq_width(16.0)
+        batch.set_schedule(mode=2, block_warps=4, ir_iters=1 if prec == 32 else 0)
+        ts = event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), args.steps, args.warmup, flush, stream)
+        S.sync_status()
+        print(json.dumps({"lean": True, "systems": len(mats), "precision": prec, "ms_per_step": sum(ts) / len(ts)}),
+              flush=True)
+        return
 
     refs = [O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k) for m, b, k in zip(mats, bs, ks)]
 
@@ -733,6 +744,10 @@ def main():
     ap.add_argument("--fixed-class", type=int, default=-1, help="use this schedule class instead of selecting one")
     ap.add_argument("--lean", type=int, default=0, choices=[0, 32, 64],
                     help="profiling run: only the timed solves of --fixed-class at this precision")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="profiling runs (--lean) only: shrink the configuration's n by this factor")
+    ap.add_argument("--systems", type=int, default=512,
+                    help="profiling runs (--lean) of c3 only: the number of systems in the batch")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

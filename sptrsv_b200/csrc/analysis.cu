@@ -69,18 +69,25 @@ __global__ void k_validate(const int* __restrict__ rowptr, const int* __restrict
 // read from the warp's shared-memory ring; a dependency outside is polled
 // warp-convergently (level 0 = not yet written).  Row metadata of the whole
 // chunk is loaded up front, one row per lane.
+// With a task table (task_r0 != null), task t covers rows [task_r0[t],
+// task_r0[t] + task_cnt[t]) instead (at most 32 consecutive rows); any
+// order in which every row's dependencies lie in earlier tasks or earlier in
+// its own task is deadlock-free.
 __global__ void __launch_bounds__(256) k_levels(const int* __restrict__ rowptr, const int* __restrict__ col, int n,
-                                                int* level, int* nlevs, DevStatus* st, unsigned long long budget)
+                                                int* level, int* nlevs, DevStatus* st, unsigned long long budget,
+                                                const int* __restrict__ task_r0, const int* __restrict__ task_cnt,
+                                                long long ntask)
 {
     __shared__ int ring[8][32];
     const int lane = threadIdx.x & 31;
     int* my = ring[threadIdx.x >> 5];
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long ntasks = ((long long)n + 31) / 32;
+    const long long ntasks = task_r0 ? ntask : ((long long)n + 31) / 32;
     int my_max = 0;
     for (long long t = gw; t < ntasks; t += nw) {
-        const int r0 = (int)(t * 32), cnt = min(32, n - r0);
+        const int r0 = task_r0 ? __ldg(task_r0 + t) : (int)(t * 32);
+        const int cnt = task_r0 ? __ldg(task_cnt + t) : min(32, n - r0);
         int ms = 0, me = 0;
         if (lane < cnt) {
             ms = __ldg(rowptr + r0 + lane);
@@ -199,7 +206,7 @@ int validate_csr_device(const int* rowptr, const int* col, int n, int nnz, cudaS
 }
 
 // Runs the whole analysis; fills *info per `mode` and registers the record.
-int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode)
+int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode, const LevelTasks* tasks)
 {
     if (!info || !L) return set_error(SPTRSV_ERR_INVALID_ARG, "analysis: NULL info or matrix");
     const int n = L->nr;
@@ -256,8 +263,10 @@ int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode)
     int nlevs = 0;
     if (n > 0) {
         // one 32-row chunk per warp, 8 warps per block
-        ACHK(launch_persistent(k_levels, 256, 0, ((long long)n + 255) / 256, s, L->ia, L->ja, n, rec->d_levels,
-                               d_nlevs, c->d_status, wait_budget_ns()));
+        const long long nt = tasks ? tasks->n : ((long long)n + 31) / 32;
+        ACHK(launch_persistent(k_levels, 256, 0, (nt + 7) / 8, s, L->ia, L->ja, n, rec->d_levels, d_nlevs,
+                               c->d_status, wait_budget_ns(), tasks ? tasks->r0 : (const int*)nullptr,
+                               tasks ? tasks->cnt : (const int*)nullptr, nt));
         ACHK(cudaMemcpyAsync(&nlevs, d_nlevs, sizeof(int), cudaMemcpyDeviceToHost, s));
         int st = sync_status(s);
         if (st) return fail(st);

@@ -150,6 +150,16 @@ struct AnalysisRec {
     int tile_ntasks[6] = {};
 };
 void register_analysis(const int* key, AnalysisRec* rec);
+
+// Task order for the level kernel: task t covers the cnt[t] <= 32 rows from
+// r0[t]; null keeps consecutive 32-row chunks in natural order.
+struct LevelTasks {
+    const int* r0;
+    const int* cnt;
+    long long n;
+};
+// The analysis behind run_analysis / multirow_analysis_base_GPU.
+int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode, const LevelTasks* tasks = nullptr);
 AnalysisRec* find_analysis(const int* key);
 AnalysisRec* unregister_analysis(const int* key);
 

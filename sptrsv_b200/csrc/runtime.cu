@@ -120,7 +120,6 @@ __global__ void k_wait_unset_flag(const int* flag, DevStatus* st, unsigned long 
     wait_ready(flag, v, st, budget, -1);
 }
 
-int run_analysis_impl(dfr_analysis_info_t* info, const sp_mat_t* L, MODE mode);
 int solve_reference(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b, double* x, int n, MODE mode,
                     int lanes, cudaStream_t stream);
 
