@@ -842,7 +842,7 @@ int vk_grid(const sptrsv_batch_s* B, long long max_blocks, long long* g)
     const int cap = B->warps_per_sm > 0 ? (B->warps_per_sm + B->block_warps - 1) / B->block_warps : 0;
     const size_t smem = (size_t)seq_per_block(B) * SeqSmem<V, T, BT>::total;
     auto kern = k_sptrsv_vk<V, T, BT, OUT>;
-    if (smem > 48 * 1024)  // the occupancy query needs the kernel's opt-in to large shared memory
+    if (smem > 32 * 1024)  // the occupancy query needs the kernel's opt-in to large shared memory
         SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     SPT_CUDA(persistent_grid(kern, 32 * B->block_warps, smem, max_blocks, cap, g));
     return 0;
@@ -955,7 +955,7 @@ int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cu
         SPT_CUDA(cudaMemsetAsync(B->flags, 0, sizeof(int) * (size_t)B->nchunks, s));
         auto kern = k_sptrsv_vkc<V, T, BT, OUT>;
         const size_t smem = (size_t)B->block_warps * 32 * 32 * sizeof(T);
-        if (smem > 48 * 1024)
+        if (smem > 32 * 1024)
             SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(B->nchunks, B->block_warps), cap, s, nb, val, di,
                                           B->nchunks, B->flags, b, x, x64, c->d_status, wait_budget_ns(),
@@ -970,7 +970,7 @@ int batch_launch(sptrsv_batch_s* B, bool f32, const BT* b, T* x, double* x64, cu
     SeqSet q{B->nptr, B->ncol, B->sys_row0, B->sys_k, B->sys_off, B->wptr, B->wsys, B->wcol, B->nseqw};
     auto kern = k_sptrsv_vk<V, T, BT, OUT>;
     const size_t smem = B->nseqw > 0 ? (size_t)seq_per_block(B) * SeqSmem<V, T, BT>::total : 0;
-    if (smem > 48 * 1024)
+    if (smem > 32 * 1024)
         SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (B->ntasks == 0 && B->nseqw == 0) return 0;
     SPT_CUDA(launch_persistent_capped(kern, block, smem, vk_max_blocks(B, B->nseqw), cap, s, bm, val, di, B->ntasks,

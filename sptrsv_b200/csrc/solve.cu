@@ -253,11 +253,13 @@ sptrsv_schedule_t default_schedule()
     return s;
 }
 
-// Once-per-instantiation opt-in to large dynamic shared memory.
+// Opt-in to large dynamic shared memory.  The default limit covers static
+// plus dynamic shared memory up to 48 KB, so a kernel with static shared
+// memory needs the opt-in a little below that.
 template <typename K>
 cudaError_t allow_smem(K kern, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return cudaSuccess;
+    if (bytes <= 32 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 

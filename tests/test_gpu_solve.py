@@ -460,3 +460,29 @@ def test_streamed_host_solve(torch_cuda, shape):
     assert O.rel_err(hx.numpy(), ref * (1.0 + (reps - 1) % 3)) <= TOL
     plan.close()
     S.free_device_analysis(L, info)
+
+
+def test_wave_group_of_exactly_48k_shared_memory(torch_cuda):
+    """4 lines of 1536 rows per CTA: the FP64 WAVE kernel asks for exactly
+    48 KB of dynamic shared memory beside its static shared word, which needs
+    the large-shared-memory opt-in (a launch without it is refused)."""
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.grid2d(1536, 8, seed=3)
+    xt = gen.vector(m.n, "uniform", seed=4)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m, S.MULTIROW)
+    plan = S.Plan(L, info)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.empty(m.n, dtype=torch.float64, device="cuda")
+    plan.set_schedule(variant=S._lib.VAR_WAVE, block_warps=4, ir_max_iters=2)
+    plan.solve_f64(db, dx)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    plan.solve_ir(db, dx)
+    S.sync_status()
+    assert O.rel_err(dx.cpu().numpy(), ref) <= TOL
+    plan.close()
+    S.free_device_analysis(L, info)
