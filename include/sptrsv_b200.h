@@ -263,8 +263,8 @@ int sptrsv_solve_f32(sptrsv_plan_t plan, const double* b, float* x32, int nrhs, 
  * right-hand side and both host arrays pinned (cudaHostAlloc or registered),
  * the copies overlap the solve: b goes over in 1 MiB segments on a
  * plan-owned side stream while the kernel runs (it waits for each segment),
- * and the kernel writes x into host_x as rows finish.  Returns after the
- * solve. */
+ * and the kernel writes x into host_x as groups of rows finish.  Returns
+ * after the solve. */
 int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, int nrhs,
                       int precision, cudaStream_t stream);
 

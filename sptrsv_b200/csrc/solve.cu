@@ -194,8 +194,9 @@ void* mapped_host(const void* h)
 // host b and x): b goes to the device in segments on a side stream, each
 // segment followed by a 4-byte copy of the call's epoch into its flag word,
 // while the solve kernel already runs; the kernel waits for a segment's flag
-// before it reads its b, and writes x to the host array as rows finish.  The
-// side stream never waits on the kernel; the kernel's waits are bounded.
+// before it reads its b, and writes x to the host array as groups of rows
+// finish.  The side stream never waits on the kernel; the kernel's waits are
+// bounded.
 int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cudaStream_t s)
 {
     const int n = p->n;

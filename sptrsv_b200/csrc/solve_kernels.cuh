@@ -491,7 +491,9 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstr
 // word set to `epoch`; a warp waits (acquire) for the flag of a row's
 // segment before it loads that row's b (only when the row's segment differs
 // from the last one the lane confirmed), and reads b coherently.  With hx
-// set, every x value is also written to that (mapped, pinned) host array.
+// set, the CTA also writes its group's x values from shared memory to that
+// (mapped, pinned) host array in one burst once the group is done, so no
+// store to host memory sits on the line-to-line critical path.
 //
 // U entries per lane are waited for together in one round; U = 2 when no
 // row holds more than two entries outside its chunk recurrence (2D
@@ -598,13 +600,15 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                 if (md.row >= 0) {
                     xs[md.row - r0] = xi;
                     publish<T, OUT>(x, x64, md.row, xi);
-                    if (STREAM && hx) hx[md.row] = (double)xi;
                 }
             }
         }
         if (failed && lane == 0) abort_flag = 1;
         __syncthreads();
         if (abort_flag) return;
+        // each thread copies the slots it refills with the sentinel for the next group
+        if (STREAM && hx)
+            for (int t = threadIdx.x; t < nr; t += blockDim.x) hx[r0 + t] = (double)xs[t];
     }
 }
 

@@ -430,7 +430,7 @@ def test_strip_full_size_grid(torch_cuda):
 @pytest.mark.parametrize("shape", [(512, 600), (100, 77)], ids=["three_segments", "small"])
 def test_streamed_host_solve(torch_cuda, shape):
     """Host-buffer solves of a WAVE plan with pinned b and x copy b in
-    segments while the solve runs and write x to the host as rows finish: the
+    segments while the solve runs and write x to the host as line groups finish: the
     result matches the oracle call after call (the segment flags' epochs wrap
     after 255 calls, and b changes between calls), and pageable buffers take
     the plain copy path."""
