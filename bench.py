@@ -135,6 +135,56 @@ class ClockSampler:
                 "samples": len(sm), "power_w_mean": statistics.mean(pw) if pw else None}
 
 
+class EnergyMeter:
+    """Energy per solve from the GPU's cumulative energy counter (NVML
+    nvmlDeviceGetTotalEnergyConsumption, millijoules; a read-only query),
+    read before and after a loop of back-to-back solves of at least
+    `min_s` seconds: energy delta / solves in that window.  The reference
+    samples power in a thread and prints watts per solver
+    (source/nvmlPower.cpp:22-59, header/common.h:121); the counter gives the
+    energy of exactly the measured window."""
+
+    def __init__(self, torch_mod, device: int):
+        self.h = None
+        self.note = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            pr = torch_mod.cuda.get_device_properties(device)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except pynvml.NVMLError:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.nvml = pynvml
+        except Exception as e:  # no NVML on this host: report why, measure nothing
+            self.note = f"NVML unavailable: {str(e)[:120]}"
+
+    def measure(self, torch_mod, fn, solves_per_call: int, min_s: float = 1.0, stream=None):
+        if self.h is None:
+            return {"note": self.note}
+        fn()
+        torch_mod.cuda.synchronize()
+        calls = 0
+        e0 = self.nvml.nvmlDeviceGetTotalEnergyConsumption(self.h)
+        t0 = time.perf_counter()
+        while True:
+            for _ in range(8):
+                fn()
+            calls += 8
+            torch_mod.cuda.synchronize()
+            if time.perf_counter() - t0 >= min_s:
+                break
+        t1 = time.perf_counter()
+        e1 = self.nvml.nvmlDeviceGetTotalEnergyConsumption(self.h)
+        joules = (e1 - e0) / 1e3
+        solves = calls * solves_per_call
+        return {"j_per_solve": joules / solves, "window_s": t1 - t0, "solves": solves,
+                "mean_power_w": joules / (t1 - t0),
+                "how": "NVML total-energy counter before/after back-to-back solves (no L2 flush)"}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -171,28 +221,52 @@ def barrier(dist):
 
 
 # ---------------------------------------------------------------- reference arm
+L2_NOTE = "flushed before every step (256 MiB write)"
+
+
+def workload_config(name: str, n: int, nnz: int, nlevs: int, k: int, world: int) -> dict:
+    """The `config` object of a single-system line; both arms print the same one."""
+    return {"workload": CONFIG_NAMES[name], "n": n, "nnz": nnz, "nlevs": nlevs, "nrhs": k, "l2": L2_NOTE,
+            "parallelism": f"replicas x{world}"}
+
+
+def batch_workload_config(mats, ks, world: int) -> dict:
+    return {"workload": CONFIG_NAMES["c3"], "systems": len(mats), "n_total": int(sum(m.n for m in mats)),
+            "nnz_total": int(sum(m.nnz for m in mats)), "rhs_total": int(sum(ks)), "l2": L2_NOTE,
+            "parallelism": f"replicas x{world}"}
+
+
+def host_flush(buf):
+    """Evicts the host caches between CPU steps (a 256 MiB write)."""
+    buf.fill(1)
+
+
 def run_reference(args, rank, world, dist):
-    """The reference's algorithm on the host cores (CPU oracle, all threads)."""
+    """The reference's algorithm on the host cores (CPU oracle, all threads).
+    Inputs come from the oracle's own copy of the generators, so this arm
+    neither imports nor loads the product library."""
     if rank != 0:
         barrier(dist)
         return
     from oracle import oracle as O
-    from sptrsv_b200 import gen
+    from oracle import workloads as W
 
     if args.config == "c3":
         run_reference_batch(args, world, dist)
         return
-    m, xt, k = gen.config(args.config)
+    m, xt, k = W.config(args.config)
     b = m.matvec(xt, k)
     a = O.analysis(m.rowptr, m.colidx)
     lev_ptr = np.concatenate([[0], np.cumsum(np.bincount(a["levels"] - 1, minlength=a["nlevs"]))]).astype(np.int32)
     threads = O.num_threads()
     x = O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
     err = O.rel_err(x, O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k))
+    flush_buf = np.empty(256 << 20, dtype=np.uint8)
     for _ in range(args.warmup):
         O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
     times = []
     for _ in range(args.steps):
+        host_flush(flush_buf)
         t0 = time.perf_counter()
         O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
         times.append(time.perf_counter() - t0)
@@ -203,7 +277,7 @@ def run_reference(args, rank, world, dist):
         "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": CONFIG_NAMES[args.config], "n": m.n, "nnz": m.nnz, "nrhs": k},
+        "config": workload_config(args.config, m.n, m.nnz, a["nlevs"], k, world),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gb_s": algorithmic_bytes(m.n, m.nnz, k) * v / 1e9, "rel_err_vs_serial": err,
@@ -217,18 +291,20 @@ def run_reference_batch(args, world, dist):
     FP64 substitution on all threads, systems one after another; a step is a
     bounded sample (systems in order until about 2 s), value = RHS solved / s."""
     from oracle import oracle as O
-    from sptrsv_b200 import gen
+    from oracle import workloads as W
 
-    mats, ks, xs = gen.batch_config(512, seed=3)
+    mats, ks, xs = W.batch_config(512, seed=3)
     threads = O.num_threads()
     prep = []
     for m, x, k in zip(mats, xs, ks):
         a = O.analysis(m.rowptr, m.colidx)
         lev_ptr = np.concatenate([[0], np.cumsum(np.bincount(a["levels"] - 1, minlength=a["nlevs"]))]).astype(np.int32)
         prep.append((m, m.matvec(x, k), k, a, lev_ptr))
+    flush_buf = np.empty(256 << 20, dtype=np.uint8)
 
     def step():
         done, t = 0, 0.0
+        host_flush(flush_buf)
         for m, b, k, a, lp in prep:
             t0 = time.perf_counter()
             O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lp, a["nlevs"], k)
@@ -251,7 +327,7 @@ def run_reference_batch(args, world, dist):
         "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": CONFIG_NAMES["c3"], "systems": len(mats), "rhs_total": int(sum(ks))},
+        "config": batch_workload_config(mats, ks, world),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -298,8 +374,8 @@ def reference_kernels(cfg: str, timeout_s: int = 240):
 
     code = (
         "import sys, json; sys.path.insert(0, %r)\n"
-        "from oracle import oracle as O\nfrom sptrsv_b200 import gen\n"
-        "m, xt, k = gen.config(%r)\nb = m.matvec(xt, k)\nref = O.solve(m.rowptr, m.colidx, m.val, b)\nout = {}\n"
+        "from oracle import oracle as O\nfrom oracle import workloads as W\n"
+        "m, xt, k = W.config(%r)\nb = m.matvec(xt, k)\nref = O.solve(m.rowptr, m.colidx, m.val, b)\nout = {}\n"
         "try:\n"
         "    x, ms, am = O.cusparse_solve(m.rowptr, m.colidx, m.val, b, reps=5)\n"
         "    out['cusparse_spsv'] = {'ms': ms, 'analysis_ms': am, 'rel_err': O.rel_err(x, ref)}\n"
@@ -519,12 +595,10 @@ def run_ours(args, rank, world, local, dist):
         "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if mode == 64 else "f32+f64-refine", "data": "synthetic",
-        "config": {"workload": CONFIG_NAMES[args.config], "n": n, "nnz": nnz, "nlevs": info.nlevs, "nrhs": k,
-                   "l2": "flushed before every step (256 MiB write)",
-                   "schedule": dict(SEL.schedule_from_class(sel64 if mode == 64 else sel32).as_dict(),
-                                    ir_max_iters=ir_iters, name=SEL.class_name(sel64 if mode == 64 else sel32)),
-                   "selected_by": "learned selector (MLP)" if learned else "exhaustive autotuner",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(args.config, n, nnz, info.nlevs, k, world),
+        "schedule": dict(SEL.schedule_from_class(sel64 if mode == 64 else sel32).as_dict(),
+                         ir_max_iters=ir_iters, name=SEL.class_name(sel64 if mode == 64 else sel32)),
+        "selected_by": "learned selector (MLP)" if learned else "exhaustive autotuner",
         "gb_s": gbs, "hbm_frac": gbs / peak,
         "rel_err": {"tuned": errs[mode], "fp64": errs[64], "fp32_refine": errs[32], "plain_fp64": err_plain,
                     "e2e": err_e2e, "tol": TOL},
@@ -701,13 +775,11 @@ def run_batch(args, rank, world, local, dist):
         "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == 64 else "f32+f64-refine", "data": "synthetic",
-        "config": {"workload": CONFIG_NAMES["c3"], "systems": len(mats), "n_total": batch.n,
-                   "nnz_total": int(sum(m.nnz for m in mats)), "rhs_total": nk, "nlevs_union": batch.nlevs,
-                   "l2": "flushed before every step (256 MiB write)",
-                   "schedule": {"mode": ["level", "chunk", "hybrid"][mode], "seq_width": width, "block_warps": bw,
-                                "ir_iters": iters, "sequential_systems": nseq, "sequential_warps": nseqw,
-                                "level_rows": nlvl},
-                   "selected_by": "exhaustive batch autotune", "parallelism": f"replicas x{world}"},
+        "config": batch_workload_config(mats, ks, world),
+        "schedule": {"mode": ["level", "chunk", "hybrid"][mode], "seq_width": width, "block_warps": bw,
+                     "ir_iters": iters, "sequential_systems": nseq, "sequential_warps": nseqw,
+                     "level_rows": nlvl, "nlevs_union": batch.nlevs},
+        "selected_by": "exhaustive batch autotune",
         "gb_s": nbytes / (ms_per_step / 1e3) / 1e9, "hbm_frac": nbytes / (ms_per_step / 1e3) / 1e9 / peak,
         "rel_err": {"tuned": err, "plain_fp64": err_plain, "e2e": err_e2e, "tol": TOL},
         "autotune_ms": {f"{['level', 'chunk', 'hybrid'][c[0]]}/w{c[1]:g}/bw{c[2]}/p{c[3]}/ir{c[4]}": v[0]

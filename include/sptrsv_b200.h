@@ -278,13 +278,22 @@ int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, do
  * arena, or that must not call cudaMalloc after start-up.  The caller passes
  * the device CSR (diagonal last), b and x (DEVICE, n values); no analysis or
  * plan is needed.  FP32 solve in natural-order chunks, then ir_iters
- * refinement steps (FP64 residual, FP32 correction, x += d in FP64).
+ * (0..16; others give SPTRSV_ERR_INVALID_ARG) refinement steps (FP64
+ * residual, FP32 correction, x += d in FP64).  The CSR is not checked on the
+ * host: the kernels check every row range and column before they use it, and
+ * a CSR that is not lower triangular with the diagonal last gives
+ * SPTRSV_ERR_INVALID_CSR.
  * Scratch lives in a fixed file-scope device array (two FP32 vectors of
- * SPTRSV_NOALLOC_MAX_ROWS and a status word; about 8 MiB on every GPU that
- * loads the library, kept until exit): n above SPTRSV_NOALLOC_MAX_ROWS is
- * rejected with SPTRSV_ERR_UNSUPPORTED.  The first call on a device looks up
- * the array's device address (make that first call before any stream
- * capture).  All calls share the array: calls that overlap on the GPU race.
+ * SPTRSV_NOALLOC_MAX_ROWS and a status word, about 8 MiB per GPU, kept until
+ * the process exits): n above SPTRSV_NOALLOC_MAX_ROWS is rejected with
+ * SPTRSV_ERR_UNSUPPORTED.  CUDA loads a library's device code lazily by
+ * default, so the array is reserved on a device when this module is first
+ * loaded there — at the first call of this function on that device (or at
+ * context creation with CUDA_MODULE_LOADING=EAGER).  That first call also
+ * looks up the array's device address.  Make it at start-up, before the
+ * pool or arena takes the device heap and before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams or
+ * host threads) race, so the caller serialises them.
  * Waits for `stream` and returns 0 or a negative SPTRSV_ERR_* code. */
 #define SPTRSV_NOALLOC_MAX_ROWS (1 << 20)
 int sptrsv_solve_ir_noalloc(const sp_mat_t* gpu_L, const double* b, double* x, int ir_iters,

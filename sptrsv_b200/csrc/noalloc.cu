@@ -56,18 +56,32 @@ int scratch_address(unsigned char** out, int* sms)
     return 0;
 }
 
-// r = b - L x over the caller's natural-order CSR (FP64), r rounded to FP32
+// r = b - L x over the caller's natural-order CSR (FP64), r rounded to FP32.
+// The CSR is checked as it is read: a row range outside [0, nnz] or a column
+// outside [0, i] records SPTRSV_ERR_INVALID_CSR and that row (or entry) is
+// skipped, so no bad index is ever used.
 __global__ void __launch_bounds__(256) k_residual_nat(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                      const double* __restrict__ val, int n,
+                                                      const double* __restrict__ val, int n, int nnz,
                                                       const double* __restrict__ b, const double* __restrict__ x,
-                                                      float* __restrict__ r)
+                                                      float* __restrict__ r, DevStatus* st)
 {
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
         const int s = rowptr[i], e = rowptr[i + 1];
+        if (!(s >= 0 && s < e && e <= nnz)) {
+            if (lane == 0) report(st, SPTRSV_ERR_INVALID_CSR, (int)i);
+            continue;
+        }
         double acc = 0.0;
-        for (int p = s + lane; p < e; p += 32) acc += val[p] * x[col[p]];
+        for (int p = s + lane; p < e; p += 32) {
+            const int c = col[p];
+            if (c < 0 || c > i) {
+                report(st, SPTRSV_ERR_INVALID_CSR, (int)i);
+                continue;
+            }
+            acc += val[p] * x[c];
+        }
         for (int o = 16; o >= 1; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) r[i] = (float)(b[i] - acc);
     }
@@ -79,7 +93,7 @@ template <typename BT, int OUT>
 cudaError_t launch_chunk(const NatMat& m, int n, const BT* b, float* x32, double* x, DevStatus* st, int sms,
                          cudaStream_t s)
 {
-    auto kern = k_sptrsv_chunk<NatMat, float, BT, OUT>;
+    auto kern = k_sptrsv_chunk<NatMat, float, BT, OUT, true>;
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
     if (e != cudaSuccess) return e;
@@ -108,7 +122,8 @@ using namespace sptrsv;
 extern "C" int sptrsv_solve_ir_noalloc(const sp_mat_t* L, const double* b, double* x, int ir_iters,
                                        cudaStream_t stream)
 {
-    if (!L || !b || !x || ir_iters < 0 || ir_iters > 16 || L->nr < 0 || L->nc != L->nr)
+    if (!L || !b || !x || ir_iters < 0 || ir_iters > 16 || L->nr < 0 || L->nc != L->nr || L->nnz < L->nr ||
+        (L->nr > 0 && (!L->ia || !L->ja || !L->a)))
         return set_error(SPTRSV_ERR_INVALID_ARG, "solve_ir_noalloc: bad arguments");
     if ((long long)L->nr > kNoallocMaxRows)
         return set_error(SPTRSV_ERR_UNSUPPORTED,
@@ -126,12 +141,12 @@ extern "C" int sptrsv_solve_ir_noalloc(const sp_mat_t* L, const double* b, doubl
     // the array keeps the previous call's contents: reset what must start clean
     SPT_CUDA(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream));
     SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)n, stream));
-    NatMat m{L->ia, L->ja, L->a, nullptr};
+    NatMat m{L->ia, L->ja, L->a, nullptr, L->nnz};
     SPT_CUDA((launch_chunk<double, OUT_SET64>(m, n, b, x32, x, st, sms, stream)));
     long long rgrid = ((long long)n * 32 + 255) / 256;  // one warp per row, at most 16 blocks per SM
     if (rgrid > 16LL * sms) rgrid = 16LL * sms;
     for (int it = 0; it < ir_iters; it++) {
-        k_residual_nat<<<(int)rgrid, 256, 0, stream>>>(L->ia, L->ja, L->a, n, b, x, r32);
+        k_residual_nat<<<(int)rgrid, 256, 0, stream>>>(L->ia, L->ja, L->a, n, L->nnz, b, x, r32, st);
         SPT_CUDA(cudaGetLastError());
         SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)n, stream));
         SPT_CUDA((launch_chunk<float, OUT_ADD64>(m, n, r32, x32, x, st, sms, stream)));
@@ -139,6 +154,9 @@ extern "C" int sptrsv_solve_ir_noalloc(const sp_mat_t* L, const double* b, doubl
     DevStatus h{};
     SPT_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
     SPT_CUDA(cudaStreamSynchronize(stream));
+    if (h.code == SPTRSV_ERR_INVALID_CSR)
+        return set_error(SPTRSV_ERR_INVALID_CSR,
+                         "solve_ir_noalloc: row %d is not lower-triangular CSR with the diagonal last", h.row);
     if (h.code == SPTRSV_ERR_TIMEOUT)
         return set_error(SPTRSV_ERR_TIMEOUT, "solve_ir_noalloc: device wait ran out of budget at row %d", h.row);
     if (h.code != 0) return set_error(h.code, "solve_ir_noalloc: device error %d at row %d", h.code, h.row);

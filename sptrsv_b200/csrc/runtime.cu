@@ -207,6 +207,18 @@ int allocate_memory(int* csrRowPtrL, int* csrColIdxL, VALUE_TYPE* csrValL, int n
     return ok();
 }
 
+// A struct that still holds an analysis made by this library (its row_ctr
+// is a registered key) owns device arrays: release them before the struct
+// is overwritten, so analysing into the same struct again leaks nothing.
+// Anything else in the struct (a fresh or uninitialised one) is only cleared.
+static void release_held_analysis(dfr_analysis_info_t* info)
+{
+    MODE m = info->mode;
+    if (info->row_ctr && find_analysis(info->row_ctr)) free_device_analysis(nullptr, info);
+    memset(info, 0, sizeof(*info));
+    info->mode = m;
+}
+
 // header/interface.h:7 — analysis per info->mode.
 int run_analysis(dfr_analysis_info_t* info, sp_mat_t* gpu_L)
 {
@@ -215,7 +227,7 @@ int run_analysis(dfr_analysis_info_t* info, sp_mat_t* gpu_L)
     if (info->mode != ORDER && info->mode != MULTIROW && info->mode != ALL)
         return set_error(SPTRSV_ERR_INVALID_ARG, "run_analysis: unknown mode %d", (int)info->mode);
     MODE m = info->mode;
-    memset(info, 0, sizeof(*info));
+    release_held_analysis(info);
     info->mode = m;
     return run_analysis_impl(info, gpu_L, m);
 }
@@ -227,7 +239,12 @@ void multirow_analysis_base_GPU(dfr_analysis_info_t** info, sp_mat_t* gpu_L, MOD
         set_error(SPTRSV_ERR_INVALID_ARG, "multirow_analysis_base_GPU: *info must point to a caller-allocated struct");
         return;
     }
-    memset(*info, 0, sizeof(**info));
+    if (!gpu_L) {
+        set_error(SPTRSV_ERR_INVALID_ARG, "multirow_analysis_base_GPU: NULL matrix");
+        return;
+    }
+    release_held_analysis(*info);
+    (*info)->mode = mode;
     run_analysis_impl(*info, gpu_L, mode);
 }
 

@@ -40,6 +40,7 @@ struct NatMat {
     const int* __restrict__ col;
     const double* __restrict__ val;
     const int* __restrict__ seq;  // null: natural order
+    int nnz;                      // entries of col/val; read only by kernels that check the CSR
     typedef double V;
     __device__ __forceinline__ RowRef row(int pos) const
     {
@@ -618,7 +619,15 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
 // solved by this warp a moment ago and is read from the warp's shared-memory
 // ring without waiting; others are polled warp-convergently.  The next row's
 // metadata and first elements are loaded while the current row waits.
-template <class M, typename T, typename BT, int OUT>
+//
+// CHECK (NatMat only; for callers whose CSR was never validated on the host):
+// before a row's entries are touched, its range must satisfy
+// 0 <= rowptr[r] < rowptr[r+1] <= nnz with the diagonal last
+// (col[rowptr[r+1]-1] == r), and every off-diagonal column must satisfy
+// 0 <= c < r before it indexes the ring or x.  A violation records
+// SPTRSV_ERR_INVALID_CSR and the row in the status word and the warp leaves
+// without any access through the bad index.
+template <class M, typename T, typename BT, int OUT, bool CHECK = false>
 __global__ void __launch_bounds__(512) k_sptrsv_chunk(M m, int n, int R, const BT* __restrict__ b, T* x, double* x64,
                                                       DevStatus* st, unsigned long long budget, unsigned backoff)
 {
@@ -632,11 +641,23 @@ __global__ void __launch_bounds__(512) k_sptrsv_chunk(M m, int n, int R, const B
         const int r0 = t * R, cnt = min(R, n - r0);
         // row j of the chunk: metadata in lane j (cnt <= 32)
         RowRef mq;
+        mq.s = mq.e = 0;
         T mpiv = 0, mb = 0;
+        bool bad = false;
         if (lane < cnt) {
             mq = m.row(r0 + lane);
-            mpiv = (T)m.inv(mq);
-            mb = (T)b[mq.r];
+            if constexpr (CHECK) bad = !(mq.s >= 0 && mq.s <= mq.e && mq.e < m.nnz) || m.c(mq.e) != mq.r;
+            if (!bad) {
+                mpiv = (T)m.inv(mq);
+                mb = (T)b[mq.r];
+            }
+        }
+        if constexpr (CHECK) {
+            const unsigned badm = __ballot_sync(0xffffffffu, bad);
+            if (badm) {
+                if (lane == __ffs(badm) - 1) report(st, SPTRSV_ERR_INVALID_CSR, mq.r);
+                return;
+            }
         }
         int ns = __shfl_sync(0xffffffffu, mq.s, 0), ne = __shfl_sync(0xffffffffu, mq.e, 0);
         int nc = 0;
@@ -665,6 +686,13 @@ __global__ void __launch_bounds__(512) k_sptrsv_chunk(M m, int n, int R, const B
                 if (have && !first) {
                     c = m.c(p);
                     v = (T)m.v(p);
+                }
+                if constexpr (CHECK) {
+                    const unsigned badm = __ballot_sync(0xffffffffu, have && (c < 0 || c >= r0 + j));
+                    if (badm) {
+                        if (lane == __ffs(badm) - 1) report(st, SPTRSV_ERR_INVALID_CSR, r0 + j);
+                        return;
+                    }
                 }
                 const bool local = have && c >= r0;
                 T xv = local ? my[c - r0] : (T)0;

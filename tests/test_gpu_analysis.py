@@ -142,3 +142,38 @@ def test_bounded_wait_times_out_and_context_survives(torch_cuda):
     m = gen.banded(3000, 32, 1, 6, seed=9)
     got = _analyse(S, m, S.MULTIROW)
     _compare(got, O.analysis(m.rowptr, m.colidx))
+
+
+@pytest.mark.parametrize("mode_name", ["ORDER", "MULTIROW"])
+def test_multirow_analysis_base_gpu_entry_point(torch_cuda, mode_name):
+    """header/analysis.h:20 called by its own name: bit-exact with the oracle
+    and with run_analysis, and analysing into the same struct again releases
+    the arrays the struct held (no device memory leaks across re-analyses)."""
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    mode = getattr(S, mode_name)
+    m = gen.banded(200_000, 256, 8, 8, seed=31)
+    ref = O.analysis(m.rowptr, m.colidx)
+    L = S.allocate_memory(m.rowptr, m.colidx, m.val, m.n)
+    info = S.AnalysisInfo()
+    S.multirow_analysis_base_GPU(info, L, mode)
+    assert info.mode == mode
+    got = S.analysis_arrays(info, m.n)
+    _compare(got, ref, warp_map=mode == S.MULTIROW)
+    assert np.array_equal(got["iorder"], _analyse(S, m, mode)["iorder"])
+    # the same struct analysed again, several times: device memory stays flat
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(6):
+        S.multirow_analysis_base_GPU(info, L, mode)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < 4 << 20, (free0, free1)
+    _compare(S.analysis_arrays(info, m.n), ref, warp_map=mode == S.MULTIROW)
+    # a plan built on the re-analysed struct solves correctly
+    b = m.matvec(gen.vector(m.n, "uniform", seed=32))
+    x = np.zeros(m.n)
+    S.run_solver(L, info, b, x, m.n)
+    assert O.rel_err(x, O.solve(m.rowptr, m.colidx, m.val, b)) <= 1e-12
+    S.free_device_analysis(L, info)

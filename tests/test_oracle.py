@@ -173,3 +173,28 @@ def test_oracle_matches_reference_golden(path):
     if "ref_x_unit_multirow" in g:
         for v in ("simple", "order", "multirow"):
             assert np.all(g[f"ref_x_unit_{v}"] == 1.0), v
+
+
+@pytest.mark.parametrize("name,scale", [("c0", 0.05), ("c1", 0.01), ("c2", 0.002), ("c2k16", 0.002)])
+def test_oracle_workloads_match_library_generators(name, scale):
+    """The CPU baseline builds its inputs through the oracle library; they must
+    be the very matrices and vectors the GPU arm solves."""
+    from oracle import workloads as W
+
+    m1, x1, k1 = gen.config(name, scale)
+    m2, x2, k2 = W.config(name, scale)
+    assert k1 == k2
+    for a, b in ((m1.rowptr, m2.rowptr), (m1.colidx, m2.colidx), (m1.val, m2.val), (x1, x2)):
+        assert np.array_equal(a, b)
+    assert np.array_equal(m1.matvec(x1, k1), m2.matvec(x2, k2))
+
+
+def test_oracle_batch_workload_matches_library_generator():
+    from oracle import workloads as W
+
+    a = gen.batch_config(6, seed=3, n_hi=3000)
+    b = W.batch_config(6, seed=3, n_hi=3000)
+    assert a[1] == b[1]
+    for m1, m2, x1, x2 in zip(a[0], b[0], a[2], b[2]):
+        assert np.array_equal(m1.rowptr, m2.rowptr) and np.array_equal(m1.colidx, m2.colidx)
+        assert np.array_equal(m1.val, m2.val) and np.array_equal(x1, x2)
