@@ -71,6 +71,19 @@ struct WaveLayout {
     int maxe = 0;                      // most entries of one slot
 };
 
+// Multi-RHS task table for kp = 1 << j lanes per row (built on demand, see
+// mrhs.cu): 8 ints per task (MrhsTask), level-aligned, each level's pieces of
+// long rows first, then its groups of short rows.
+struct MrhsTable {
+    int* tasks = nullptr;   // [ntasks * 8]
+    int ntasks = 0;
+    int npslots = 0;        // partial-sum slots (pieces of rows cut in more than one piece)
+    int nsplit = 0;         // rows cut in more than one piece (one counter each)
+    void* pbuf = nullptr;   // [npslots * kp] partial sums (f64; f32 solves use the front half)
+    int* pcnt = nullptr;    // [nsplit] piece counters, cleared before each launch
+    int U = 0;              // elements per lane per wait round the table was cut for
+};
+
 struct sptrsv_plan_s {
     int device = -1;
     int n = 0, nnz_off = 0, nlevs = 0, n_warps = 0;
@@ -88,6 +101,7 @@ struct sptrsv_plan_s {
     int* clu_tasks = nullptr;    // (cluster, level)-aligned tasks
     int* clu_ctask = nullptr;    // first task of each cluster [nclusters+1]
     int clu_ntasks = 0, clu_R = 0;
+    MrhsTable mrhs[6];           // multi-RHS tables per kp = 1 << j (built on demand)
     StripLayout strip;           // STRIP layout (built on demand)
     int row_strip_R = 0;         // R the strip layout was built for (0: none)
     WaveLayout wave;             // WAVE layout (built on demand)
@@ -128,4 +142,7 @@ void strip_free(StripLayout& t);
 // max_rows.
 int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows);
 void wave_free(WaveLayout& w);
+// Builds (or keeps) the multi-RHS task table for kp lanes per row.
+int build_mrhs_tasks(sptrsv_plan_s* p, int kp, int U);
+void mrhs_free(MrhsTable& t);
 }  // namespace sptrsv

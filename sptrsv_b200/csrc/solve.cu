@@ -167,7 +167,10 @@ void plan_free_arrays(sptrsv_plan_s* p)
     strip_free(p->strip);
     wave_free(p->wave);
     cudaFree(p->cptr); cudaFree(p->inv); cudaFree(p->levels); cudaFree(p->ibase); cudaFree(p->ivect);
-    for (int j = 0; j < 6; j++) cudaFree(p->ord_tasks[j]);
+    for (int j = 0; j < 6; j++) {
+        cudaFree(p->ord_tasks[j]);
+        mrhs_free(p->mrhs[j]);
+    }
     cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
     cudaFree(p->w32a); cudaFree(p->w32b); cudaFree(p->hb); cudaFree(p->hx);
     cudaFree(p->bflag);
@@ -390,18 +393,31 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
                  sc.variant == SPTRSV_VAR_SIMPLE ? p->inv : nullptr};
     const int wpb = sc.block_warps;
     if (nrhs > 1) {
-        // multi-RHS: level-aligned tasks of 32/kp rows over the level layout
+        // multi-RHS: level-aligned groups of short rows and pieces of long rows
         PermMat<V> ml = m;
         ml.seq = nullptr;
         int kp = 1, j = 0;
         while (kp < nrhs) kp <<= 1;
-        int e = build_order_tasks(p, 32 / kp);
+        while ((1 << j) < kp) j++;
+        // entries per lane per wait round (the table's round size): 16 where levels
+        // are wide and the gathers in flight set the pace, 8 where levels are
+        // narrow and more resident warps (fewer registers) shorten each hop
+        // (measured on B200: Zipf n = 2e6, 16 RHS 3.98 vs 4.53 ms; banded
+        // n = 1e5, 16 RHS 4.67 vs 6.53 ms)
+        const int U = (long long)p->n >= 1024LL * std::max(1, p->nlevs) ? 16 : 8;
+        int e = build_mrhs_tasks(p, kp, U);
         if (e) return e;
-        while ((1 << j) < 32 / kp) j++;
-        auto kern = k_sptrsv_mrhs<PermMat<V>, T, BT, OUT>;
-        SPT_CUDA(launch_persistent_capped(kern, block, 0, div_up(p->ord_ntasks[j], wpb), cap, s, ml,
-                                          p->ord_ntasks[j], (const int*)p->ord_tasks[j], nrhs, kp, b, x, x64,
-                                          c->d_status, budget, backoff));
+        const MrhsTable& t = p->mrhs[j];
+        if (t.nsplit) SPT_CUDA(cudaMemsetAsync(t.pcnt, 0, sizeof(int) * (size_t)t.nsplit, s));
+        // rows of x a whole number of 16-byte copies wide: gathered through L2 in 16-byte copies
+        const bool cg = (nrhs * sizeof(T)) % 16 == 0;
+        auto kern = U == 8 ? (cg ? k_sptrsv_mrhs<V, T, BT, OUT, 8, MRHS_CG> : k_sptrsv_mrhs<V, T, BT, OUT, 8, MRHS_CA>)
+                           : (cg ? k_sptrsv_mrhs<V, T, BT, OUT, 16, MRHS_CG> : k_sptrsv_mrhs<V, T, BT, OUT, 16, MRHS_CA>);
+        const size_t smem = (size_t)wpb * U * 32 * sizeof(T);
+        SPT_CUDA(allow_smem(kern, smem));
+        SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(t.ntasks, wpb), cap, s, ml, t.ntasks,
+                                          reinterpret_cast<const MrhsTask*>(t.tasks), nrhs, kp, b, x, x64,
+                                          reinterpret_cast<T*>(t.pbuf), t.pcnt, c->d_status, budget, backoff));
         return 0;
     }
     if (sc.variant == SPTRSV_VAR_SIMPLE) {

@@ -291,54 +291,270 @@ __global__ void __launch_bounds__(512) k_sptrsv_cluster(PermMat<V> m, const int*
     }
 }
 
-// nrhs right-hand sides (row-major n x K).  kp = power of two >= K lanes per
-// row; level-aligned task t covers positions [tbase[t], tbase[t+1]) (at
-// most 32/kp rows); lane k of a row owns right-hand side k and walks all of
-// the row's elements, kMrhsU per round: their columns, then their x values,
-// are loaded back to back and the warp waits for the round together.  The
-// products are subtracted in element order.
-constexpr int kMrhsU = 8;
-template <class M, typename T, typename BT, int OUT>
-__global__ void __launch_bounds__(512, 1) k_sptrsv_mrhs(M m, int ntasks, const int* __restrict__ tbase, int K, int kp,
-                                                     const BT* __restrict__ b, T* x, double* x64, DevStatus* st,
-                                                     unsigned long long budget, unsigned backoff)
+// nrhs right-hand sides (row-major n x K), kp = power of two >= K lanes per
+// row.  Level-aligned tasks of two kinds (table built by build_mrhs_tasks):
+//
+//   GROUP  {pos, cnt > 0, s0, lens[0..7], lens[8..15]}: the cnt <= E = 32/kp
+//          short rows at positions [pos, pos+cnt), whose entries are the
+//          contiguous range from s0; row j holds 4-bit lens[j] <= U entries.
+//          Row seg takes lanes seg*kp .. seg*kp+kp-1; lane k owns right-hand
+//          side k and handles all of its row's entries in one wait round.
+//   PIECE  {pos, -npieces, e0, e1, pslot, cslot, piece}: entries [e0, e1) of
+//          the long row at pos.  The warp's lanes are E element slots x kp
+//          right-hand sides: slot e takes entries e0+e, e0+e+E, ..., U per
+//          wait round, so each entry's K-wide line of x is one coalesced
+//          gather; the slots' partial sums are added by shuffles.  A row of
+//          one piece publishes x directly; otherwise each piece stores its
+//          partial sums in pbuf[pslot] and bumps the row's counter
+//          pcnt[cslot]; the piece that bumps it last adds all of the row's
+//          partials in piece order (deterministic) and publishes x.
+//
+// The solve is bound by how many x gathers are in flight (the memory system,
+// not the arithmetic, sets the pace), so the x values of a round are copied
+// into the warp's shared-memory slots with cp.async: U = 16 gathers per lane
+// in flight without holding registers for them.  A copied value equal to the
+// sentinel (its row not published yet, or a stale line in L1) is re-polled
+// with ld.relaxed.gpu and written back into its slot, and the products are
+// then taken in entry order, so the sums are deterministic.  A long row
+// costs about one wait round whatever its length, and pieces of a row sit in
+// the same level, so their tasks never wait on each other.  The next task's
+// record is loaded one task ahead.
+struct MrhsTask {
+    int pos, cnt, e0, e1;  // GROUP: e0 = s0, e1 = lens of rows 0..7; PIECE: entry range
+    int pslot, cslot, piece, pad;  // GROUP: pslot = lens of rows 8..15
+};
+
+template <typename T>
+__device__ __forceinline__ T ld_cg(const T* p)
 {
-    const int lane = threadIdx.x & 31;
-    const int seg = lane / kp, k = lane & (kp - 1);
-    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-    for (int t = gw; t < ntasks; t += nw) {
-        const int base = __ldg(tbase + t), cnt = __ldg(tbase + t + 1) - base;
-        const bool act = seg < cnt && k < K;
-        RowRef q;
-        T piv = 0, acc = 0;
-        int len = 0;
-        if (act) {
-            q = m.row(base + seg);
-            piv = (T)m.inv(q);
-            acc = (T)b[(size_t)q.r * K + k];
-            len = q.e - q.s;
-        }
-        const int rounds = __reduce_max_sync(0xffffffffu, len);
-        for (int j = 0; j < rounds; j += kMrhsU) {
-            const int nh = min(kMrhsU, len - j);
-            long long ci[kMrhsU];
-            T vv[kMrhsU], xv[kMrhsU];
+    return __ldcg(p);
+}
+
+// This lane's entries of a task: first entry s, count n, stride (GROUP 1, PIECE E).
+__device__ __forceinline__ void mrhs_lane_range(const int4& h, const int4& h2, int seg, int E, int& s, int& n,
+                                                int& stride)
+{
+    if (h.y > 0) {
+        const unsigned long long lens = (unsigned)h.w | ((unsigned long long)(unsigned)h2.x << 32);
+        int off = 0;
+        for (int i = 0; i < seg; i++) off += (int)((lens >> (4 * i)) & 15u);
+        s = h.z + off;
+        n = seg < h.y ? (int)((lens >> (4 * seg)) & 15u) : 0;
+        stride = 1;
+    } else {
+        s = h.z + seg;
+        n = s < h.w ? (h.w - s + E - 1) / E : 0;
+        stride = E;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_ca(T* smem, const T* g)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(g), "n"(sizeof(T)) : "memory");
+}
+// 16 bytes through L2 only (no L1 line that could go stale while a row is pending)
+__device__ __forceinline__ void cp_async_cg16(void* smem, const void* g)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Gather modes of the multi-RHS solve.
+enum { MRHS_LD = 0, MRHS_CA = 1, MRHS_CG = 2 };
+
+// The gathers of one wait round: x[cc[u]*K + k] into xs[u*32 + lane] for the
+// lane's nh entries.  CG (K * sizeof(T) a multiple of 16 bytes): lanes with
+// k % (16/sizeof(T)) == 0 copy 16 bytes for themselves and the next lanes
+// (same row, same entries) through L2; otherwise each lane copies its value.
+template <typename T, int U, int GM>
+__device__ __forceinline__ void mrhs_gather(const int (&cc)[U], int nh, const T* xk, int K, int k, T* xs, int lane)
+{
+    constexpr int VEC = 16 / sizeof(T);
+    if (GM == MRHS_LD) {
+        T v[U];
 #pragma unroll
-            for (int u = 0; u < kMrhsU; u++) {
-                ci[u] = 0;
-                vv[u] = 0;
-                if (u < nh) {
-                    ci[u] = (long long)m.c(q.s + j + u) * K + k;
-                    vv[u] = (T)m.v(q.s + j + u);
+        for (int u = 0; u < U; u++)
+            if (u < nh) v[u] = ld_relaxed(xk + (size_t)cc[u] * K);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (u < nh) xs[u * 32 + lane] = v[u];
+        return;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        if (u < nh) {
+            if (GM == MRHS_CG) {
+                if ((k & (VEC - 1)) == 0) cp_async_cg16(xs + u * 32 + lane, xk + (size_t)cc[u] * K);
+            } else {
+                cp_async_ca(xs + u * 32 + lane, xk + (size_t)cc[u] * K);
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+}
+
+// Re-polls (ld.relaxed.gpu) the lane's gathered values that still hold the
+// sentinel, writes each into its slot once ready, then subtracts the
+// products in entry order from acc.  Returns false (warp-uniform) on timeout
+// or abort.
+template <typename T, int U>
+__device__ __forceinline__ bool mrhs_finish_round(const int (&cc)[U], const T (&vv)[U], int nh, const T* xk, int K,
+                                                  T* xs, int lane, T& acc, DevStatus* st, unsigned long long budget,
+                                                  unsigned backoff, int row)
+{
+    unsigned pend = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++)
+        if (u < nh && is_pending(xs[u * 32 + lane])) pend |= 1u << u;
+    if (__any_sync(0xffffffffu, pend != 0)) {
+        unsigned long long t0 = 0;
+        unsigned it = 0;
+        while (true) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if ((pend >> u) & 1u) {
+                    const T v = ld_relaxed(xk + (size_t)cc[u] * K);
+                    if (!is_pending(v)) {
+                        xs[u * 32 + lane] = v;
+                        pend &= ~(1u << u);
+                    }
                 }
             }
-            if (!warp_wait_n<false, kMrhsU, T>(nh, ci, x, nullptr, xv, st, budget, backoff, act ? q.r : -1)) return;
-#pragma unroll
-            for (int u = 0; u < kMrhsU; u++)
-                if (u < nh) acc -= vv[u] * xv[u];
+            if (!__any_sync(0xffffffffu, pend != 0)) break;
+            ++it;
+            if (backoff && it > 8) __nanosleep(backoff);
+            if ((it & 63u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                    unsigned long long now = global_ns();
+                    if (t0 == 0) t0 = now;
+                    if (ld_relaxed(&st->code) != 0) stop = 1;
+                    else if (now - t0 > budget) {
+                        report(st, SPTRSV_ERR_TIMEOUT, row);
+                        stop = 1;
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, stop, 0)) return false;
+            }
         }
-        if (act) publish<T, OUT>(x, x64, (size_t)q.r * K + k, acc * piv);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+        if (u < nh) acc -= vv[u] * xs[u * 32 + lane];
+    __syncwarp();  // the slots are reused by the next round
+    return true;
+}
+
+template <class M, typename T, int U>
+__device__ __forceinline__ void mrhs_load_round(const M& m, int s, int stride, int nh, int (&cc)[U], T (&vv)[U])
+{
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        cc[u] = 0;
+        vv[u] = 0;
+        if (u < nh) {
+            cc[u] = m.c(s + u * stride);
+            vv[u] = (T)m.v(s + u * stride);
+        }
+    }
+}
+
+template <typename V, typename T, typename BT, int OUT, int U, int GM>
+__global__ void __launch_bounds__(256) k_sptrsv_mrhs(PermMat<V> m, int ntasks, const MrhsTask* __restrict__ tasks,
+                                                     int K, int kp, const BT* __restrict__ b, T* x, double* x64,
+                                                     T* pbuf, int* pcnt, DevStatus* st, unsigned long long budget,
+                                                     unsigned backoff)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int seg = lane / kp, k = lane & (kp - 1), E = 32 / kp;
+    const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    const bool kok = k < K;
+    const T* xk = x + k;
+    T* xs = reinterpret_cast<T*>(smem_raw) + (size_t)wib * U * 32;
+    const int4* rec = reinterpret_cast<const int4*>(tasks);
+    int t = gw;
+    if (t >= ntasks) return;
+    // Per task: record h/h2, this lane's entry range, row id and reciprocal
+    // diagonal, and the first round's columns and values -- all issued at the
+    // end of the previous task (or here for the first one).
+    int4 h = __ldg(rec + 2 * (size_t)t), h2 = __ldg(rec + 2 * (size_t)t + 1);
+    int s, n, stride;
+    mrhs_lane_range(h, h2, seg, E, s, n, stride);
+    int rr = __ldg(m.rowid + (h.y > 0 ? h.x + min(seg, h.y - 1) : h.x));
+    T piv = (T)__ldg(m.di + (h.y > 0 ? h.x + min(seg, h.y - 1) : h.x));
+    int cc[U];
+    T vv[U];
+    int nh = kok ? min(U, n) : 0;
+    mrhs_load_round<PermMat<V>, T, U>(m, s, stride, nh, cc, vv);
+    while (true) {
+        const int tn = t + nw;
+        int4 g = h, g2 = h2;
+        if (tn < ntasks) {  // the next record, in flight while this task runs
+            g = __ldg(rec + 2 * (size_t)tn);
+            g2 = __ldg(rec + 2 * (size_t)tn + 1);
+        }
+        const bool group = h.y > 0;
+        const bool out = group ? (seg < h.y && kok) : (seg == 0 && kok);
+        const size_t xi = (size_t)rr * K + k;
+        const T bval = out ? (T)b[xi] : (T)0;  // used at publish time
+        T acc = 0;  // minus the sum of this lane's products
+        mrhs_gather<T, U, GM>(cc, nh, xk, K, k, xs, lane);
+        if (!mrhs_finish_round<T, U>(cc, vv, nh, xk, K, xs, lane, acc, st, budget, backoff, rr)) return;
+        // later rounds (pieces cut longer than one round), loaded on the spot
+        for (int j = U; __any_sync(FULL, kok && j < n); j += U) {
+            const int mh = kok ? max(0, min(U, n - j)) : 0;
+            mrhs_load_round<PermMat<V>, T, U>(m, s + j * stride, stride, mh, cc, vv);
+            mrhs_gather<T, U, GM>(cc, mh, xk, K, k, xs, lane);
+            if (!mrhs_finish_round<T, U>(cc, vv, mh, xk, K, xs, lane, acc, st, budget, backoff, rr)) return;
+        }
+        if (group) {
+            if (out) publish<T, OUT>(x, x64, xi, (bval + acc) * piv);
+        } else {
+            for (int o = 16; o >= kp; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+            const int npieces = -h.y;
+            if (npieces == 1) {
+                if (out) publish<T, OUT>(x, x64, xi, (bval + acc) * piv);
+            } else {
+                if (out) pbuf[(size_t)h2.x * K + k] = acc;
+                // the warp barrier orders the lanes' partial stores before lane
+                // 0's acq_rel bump (release: they are visible to whoever sees
+                // the bump; acquire: the last bumper sees every other piece's)
+                __syncwarp();
+                int last = 0;
+                if (lane == 0) last = atom_add_acq_rel(pcnt + h2.y, 1) == npieces - 1;
+                last = __shfl_sync(FULL, last, 0);
+                __syncwarp();
+                if (last) {
+                    if (out) {
+                        T sum = bval;
+                        const size_t p0 = (size_t)(h2.x - h2.z) * K + k;
+                        for (int q = 0; q < npieces; q++) sum += ld_cg(pbuf + p0 + (size_t)q * K);
+                        publish<T, OUT>(x, x64, xi, sum * piv);
+                    }
+                }
+            }
+        }
+        if (tn >= ntasks) break;
+        // issue the next task's loads; they land while this warp moves on
+        t = tn;
+        h = g;
+        h2 = g2;
+        mrhs_lane_range(h, h2, seg, E, s, n, stride);
+        const int rpos = h.y > 0 ? h.x + min(seg, h.y - 1) : h.x;
+        rr = __ldg(m.rowid + rpos);
+        piv = (T)__ldg(m.di + rpos);
+        nh = kok ? min(U, n) : 0;
+        mrhs_load_round<PermMat<V>, T, U>(m, s, stride, nh, cc, vv);
     }
 }
 
