@@ -56,6 +56,7 @@ CONFIG_NAMES = {
           "4-16 off-diagonals per row, 1-32 RHS each, one persistent launch replayed as a CUDA graph",
 }
 TOL = 1e-12
+PART_ROWS = (0, 4096)  # batch autotune: plain, and long systems cut into blocks of about 4096 rows
 SELECTOR_WEIGHTS = ROOT / "sptrsv_b200" / "selector_weights.npz"
 
 
@@ -574,10 +575,11 @@ def run_ours(args, rank, world, local, dist):
                 "traffic": load_traffic(f"{variant}_{'f64' if mode == 64 else 'f32'}_{args.config}"),
                 "kernel": kname, "algorithmic_bytes_per_launch": bytes_kern, "launch_ms": t_kern,
                 "peak_kind": peak_kind}
-    hops = chain_hop_us(torch, S, SEL)
-    roofline.update(hops)
-    roofline["latency_floor_ms"] = {"nlevs_x_smem_hop": info.nlevs * hops["smem_hop_us"] / 1e3,
-                                    "nlevs_x_l2_hop": info.nlevs * hops["l2_hop_us"] / 1e3}
+    if not args.extra:
+        hops = chain_hop_us(torch, S, SEL)
+        roofline.update(hops)
+        roofline["latency_floor_ms"] = {"nlevs_x_smem_hop": info.nlevs * hops["smem_hop_us"] / 1e3,
+                                        "nlevs_x_l2_hop": info.nlevs * hops["l2_hop_us"] / 1e3}
 
     # --- end to end through the C ABI host-buffer entry point
     hb = torch.from_numpy(b).pin_memory()
@@ -588,8 +590,11 @@ def run_ours(args, rank, world, local, dist):
     err_e2e = O.rel_err(hx.numpy(), ref)
 
     gbs = algorithmic_bytes(n, nnz, k) / (ms_per_step / 1e3) / 1e9
-    cpu = cpu_baseline_sample(m, b, k) if (rank == 0 and world == 1 and not args.no_cpu) else None
-    refk = reference_kernels(args.config) if (rank == 0 and world == 1 and not args.no_ref and k == 1) else None
+    energy = EnergyMeter(torch, local).measure(torch, solve(mode), k, min_s=0.5 if args.extra else 1.0)
+    cpu = (cpu_baseline_sample(m, b, k, budget_s=4.0 if args.extra else 10.0)
+           if (rank == 0 and world == 1 and not args.no_cpu) else None)
+    refk = (reference_kernels(args.config)
+            if (rank == 0 and world == 1 and not args.no_ref and not args.extra and k == 1) else None)
     t32 = mode_ms[32] if mode == 64 else ms_per_step
     line = {
         "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -619,16 +624,14 @@ def run_ours(args, rank, world, local, dist):
         "analysis_ms": analysis_ms,
         "e2e": {"value": world * k / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * n * k,
                 "d2h_bytes_per_step": 8 * n * k},
-        "energy_j_per_solve": (clocks["power_w_mean"] * ms_per_step / 1e3 / k
-                               if clocks and clocks.get("power_w_mean") else None),
+        "energy_j_per_solve": energy.get("j_per_solve"), "energy": energy,
         "roofline": roofline, "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks, "cpu_baseline": cpu, "reference_kernels": refk,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     plan.close()
     S.free_device_analysis(L, info)
     barrier(dist)
+    return line
 
 
 # ------------------------------------------------------------ batched workload
@@ -666,6 +669,7 @@ def run_batch(args, rank, world, local, dist):
     if args.lean:
         # profiling run: the default hybrid schedule, warm-up and the timed solves, nothing else
         prec = args.lean
+        batch.set_partition(args.part)
         batch.set_seq_width(16.0)
         batch.set_schedule(mode=2, block_warps=4, ir_iters=1 if prec == 32 else 0)
         ts = event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), args.steps, args.warmup, flush, stream)
@@ -680,31 +684,38 @@ def run_batch(args, rank, world, local, dist):
         return max(O.rel_err(xh[batch.offsets[s]:batch.offsets[s + 1]], refs[s]) for s in range(len(mats)))
 
     # --- schedule: level-ordered vs hybrid, block size, refinement steps (exhaustive, small)
+    # partitioned (long systems cut into blocks with warm-ups) and plain batches
     cands = []
-    for mode, width in ((0, 0.0), (2, 16.0), (2, 32.0)):
-        for bw in (2, 4, 8):
-            cands.append((mode, width, bw))
+    for part in PART_ROWS:
+        for mode, width in ((0, 0.0), (2, 16.0), (2, 32.0)):
+            for bw in (2, 4, 8):
+                cands.append((part, mode, width, bw))
     res = {}
-    for mode, width, bw in cands:
+    part_info = {}
+    for part, mode, width, bw in cands:
+        batch.set_partition(part)
+        if part not in part_info:
+            part_info[part] = batch.partition_info()
         batch.set_seq_width(width)
         for prec, iters in ((64, 0), (32, 1), (32, 2)):
             batch.set_schedule(mode=mode, block_warps=bw, ir_iters=iters)
             t = statistics.median(event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), 3, 1, flush,
                                                    stream))
             S.sync_status()
-            res[(mode, width, bw, prec, iters)] = (t, max_err(dx.cpu().numpy()))
+            res[(part, mode, width, bw, prec, iters)] = (t, max_err(dx.cpu().numpy()))
     ok = {c: v for c, v in res.items() if v[1] <= TOL}
     best = min(ok, key=lambda c: ok[c][0])
-    best64 = min((c for c in ok if c[3] == 64), key=lambda c: ok[c][0])
-    best32 = min((c for c in ok if c[3] == 32), key=lambda c: ok[c][0], default=None)
+    best64 = min((c for c in ok if c[4] == 64), key=lambda c: ok[c][0])
+    best32 = min((c for c in ok if c[4] == 32), key=lambda c: ok[c][0], default=None)
 
     def apply(c):
-        mode, width, bw, prec, iters = c
+        part, mode, width, bw, prec, iters = c
+        batch.set_partition(part)
         batch.set_seq_width(width)
         batch.set_schedule(mode=mode, block_warps=bw, ir_iters=iters)
 
     apply(best)
-    prec = best[3]
+    prec = best[4]
     sampler = ClockSampler(local)
     barrier(dist)
     torch.cuda.synchronize()
@@ -720,7 +731,8 @@ def run_batch(args, rank, world, local, dist):
     value = world * nk * args.steps / (total_ms / 1e3)
     nseq, nseqw, nlvl = batch.seq_systems()
 
-    # plain FP64: the level-ordered batched launch, no sequential warps
+    # plain FP64: the level-ordered batched launch, no sequential warps, no blocks
+    batch.set_partition(0)
     batch.set_seq_width(0.0)
     batch.set_schedule(mode=0, block_warps=8, ir_iters=1)
     t_plain = statistics.median(event_time_steps(torch, lambda: batch.solve(db, dx, 64), max(3, args.steps // 2), 1,
@@ -758,19 +770,22 @@ def run_batch(args, rank, world, local, dist):
     e2e_ms = reduce_max(dist, sum(te)) / len(te)
     err_e2e = max_err(hx.numpy())
 
+    energy = EnergyMeter(torch, local).measure(torch, lambda: batch.solve_graph(db, dx, prec), nk,
+                                               min_s=0.5 if args.extra else 1.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         done, t_cpu, sys_done = 0, 0.0, 0
+        budget = 4.0 if args.extra else 10.0
         for m, b, k in zip(mats, bs, ks):
             _, dt = O.timed(O.solve, m.rowptr, m.colidx, m.val, b, k)
             done += k
             t_cpu += dt
             sys_done += 1
-            if t_cpu > 10.0:
+            if t_cpu > budget:
                 break
         cpu = {"value": done / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port",
                "sample": f"serial FP64 substitution of the first {sys_done} systems ({done} RHS, {t_cpu:.1f} s)"}
-    mode, width, bw, _, iters = best
+    part, mode, width, bw, _, iters = best
     line = {
         "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -778,11 +793,12 @@ def run_batch(args, rank, world, local, dist):
         "config": batch_workload_config(mats, ks, world),
         "schedule": {"mode": ["level", "chunk", "hybrid"][mode], "seq_width": width, "block_warps": bw,
                      "ir_iters": iters, "sequential_systems": nseq, "sequential_warps": nseqw,
-                     "level_rows": nlvl, "nlevs_union": batch.nlevs},
+                     "level_rows": nlvl, "nlevs_union": batch.nlevs, "partition_block_rows": part,
+                     "partition": part_info.get(part)},
         "selected_by": "exhaustive batch autotune",
         "gb_s": nbytes / (ms_per_step / 1e3) / 1e9, "hbm_frac": nbytes / (ms_per_step / 1e3) / 1e9 / peak,
         "rel_err": {"tuned": err, "plain_fp64": err_plain, "e2e": err_e2e, "tol": TOL},
-        "autotune_ms": {f"{['level', 'chunk', 'hybrid'][c[0]]}/w{c[1]:g}/bw{c[2]}/p{c[3]}/ir{c[4]}": v[0]
+        "autotune_ms": {f"part{c[0]}/{['level', 'chunk', 'hybrid'][c[1]]}/w{c[2]:g}/bw{c[3]}/p{c[4]}/ir{c[5]}": v[0]
                         for c, v in res.items()},
         "fp64_best_ms": res[best64][0],
         "fp32_refine_best_ms": res[best32][0] if best32 else None,
@@ -791,17 +807,42 @@ def run_batch(args, rank, world, local, dist):
         "batch_create_s": create_s,
         "e2e": {"value": world * nk / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * batch.vec_len,
                 "d2h_bytes_per_step": 8 * batch.vec_len},
-        "energy_j_per_solve": (clocks["power_w_mean"] * ms_per_step / 1e3 / nk
-                               if clocks and clocks.get("power_w_mean") else None),
+        "energy_j_per_solve": energy.get("j_per_solve"), "energy": energy,
         "roofline": roofline, "gpu_launches": args.steps * (1 if prec == 64 else 1 + 2 * iters),
         "clocks": clocks, "cpu_baseline": cpu,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     batch.close()
     for d in dev:
         S.free_device_analysis(d, None)
     barrier(dist)
+    return line
+
+
+EXTRA_CONFIGS = ("c0", "c2k16", "c3")
+
+
+def config_summary(line: dict) -> dict:
+    """The figures of one configuration's line that ride along the headline."""
+    rf = line.get("roofline") or {}
+    cpu = line.get("cpu_baseline") or {}
+    out = {
+        "workload": line["config"]["workload"], "config": line["config"], "ms": line["ms_per_step"],
+        "solves_s": line["value"], "dtype": line["dtype"], "steps": line["steps"], "schedule": line.get("schedule"),
+        "selected_by": line.get("selected_by"), "rel_err": line["rel_err"], "gb_s": line.get("gb_s"),
+        "roofline": {k: rf.get(k) for k in ("achieved", "peak", "frac", "unit", "kernel", "launch_ms")},
+        "e2e_solves_s": line["e2e"]["value"], "plain_fp64": line.get("plain_fp64"),
+        "speedup_vs_plain_fp64": line.get("speedup_vs_plain_fp64"), "clocks": line.get("clocks"),
+        "energy_j_per_solve": line.get("energy_j_per_solve"),
+        "cpu_baseline": cpu or None,
+        "cpu_ms_per_solve": 1e3 / cpu["value"] if cpu.get("value") else None,
+    }
+    if "fp32_refine" in line and isinstance(line["fp32_refine"], dict):
+        out["fp32_refine_ms"] = line["fp32_refine"]["ms"]
+        out["fp64_ms"] = line["fp64_tuned"]["ms"]
+    else:
+        out["fp32_refine_ms"] = line.get("fp32_refine_best_ms")
+        out["fp64_ms"] = line.get("fp64_best_ms")
+    return out
 
 
 def main():
@@ -818,19 +859,38 @@ def main():
                     help="profiling run: only the timed solves of --fixed-class at this precision")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="profiling runs (--lean) only: shrink the configuration's n by this factor")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="c1 only: skip the other configurations measured after the headline")
+    ap.add_argument("--part", type=int, default=0,
+                    help="profiling runs (--lean) of c3 only: cut long systems into blocks of about this many rows")
     ap.add_argument("--systems", type=int, default=512,
                     help="profiling runs (--lean) of c3 only: the number of systems in the batch")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    args.extra = False
     rank, world, local, dist = dist_setup(args)
     try:
         if args.impl == "reference":
             run_reference(args, rank, world, dist)
-        elif args.config == "c3":
-            run_batch(args, rank, world, local, dist)
-        else:
-            run_ours(args, rank, world, local, dist)
+            return
+        line = (run_batch if args.config == "c3" else run_ours)(args, rank, world, local, dist)
+        if line is None:  # a profiling run printed its own line
+            return
+        if args.config == "c1" and world == 1 and not args.no_extra:
+            # the other configurations, measured in the same run (fewer steps)
+            line["configs"] = {}
+            for cfg in EXTRA_CONFIGS:
+                ea = argparse.Namespace(**vars(args))
+                ea.config, ea.steps, ea.warmup, ea.extra = cfg, min(args.steps, 10), 3, True
+                ea.no_ref = True
+                try:
+                    ex = (run_batch if cfg == "c3" else run_ours)(ea, rank, world, local, dist)
+                    line["configs"][cfg] = config_summary(ex)
+                except Exception as e:  # report, keep the headline
+                    line["configs"][cfg] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -210,7 +210,12 @@ typedef struct sptrsv_plan_s* sptrsv_plan_t;
 #define SPTRSV_VAR_WAVE      5  /* STRIP's chunks; block_warps grid lines per CTA,   */
                                 /* one warp per line, the lines' x in shared memory  */
                                 /* (their rows must fit: 25,600 rows in FP64)        */
-#define SPTRSV_N_VARIANTS    6
+#define SPTRSV_VAR_BAND      6  /* one warp per independent unit (the matrix, or a  */
+                                /* block of a partitioned schedule), level by level, */
+                                /* x in a shared-memory ring, no cross-warp waits;   */
+                                /* rows of at most 128 off-diagonals, levels of at   */
+                                /* most 128 rows on average per unit                 */
+#define SPTRSV_N_VARIANTS    7
 
 typedef struct {
     int variant;          /* SPTRSV_VAR_*                                            */
@@ -223,6 +228,14 @@ typedef struct {
     int ir_max_iters;     /* FP32+IR: refinement steps after the first FP32 solve     */
     int band_levels;      /* CLUSTER: levels per band (H)                             */
     int cluster_rows;     /* CLUSTER: rows per cluster (B, <= 8192)                   */
+    int partitions;       /* 0 or 1: solve L as one system.  P >= 2: cut the rows     */
+                          /* into P blocks solved independently by the variant above; */
+                          /* block i starts its substitution K_i rows early from a    */
+                          /* zero boundary (its warm-up), K_i chosen at plan time so  */
+                          /* that a proven bound on the effect of the dropped rows is */
+                          /* below 2^-60 relative to max|x|.  Needs a row diagonally  */
+                          /* dominant L (|L_ii| >= sum_j |L_ij|), else                */
+                          /* SPTRSV_ERR_UNSUPPORTED.  P <= 4096.                      */
 } sptrsv_schedule_t;
 
 /* Creates a plan for the analysed matrix.  info must come from run_analysis
@@ -231,6 +244,13 @@ int sptrsv_plan_create(const sp_mat_t* gpu_L, const dfr_analysis_info_t* info, s
 int sptrsv_plan_destroy(sptrsv_plan_t plan);
 int sptrsv_plan_set_schedule(sptrsv_plan_t plan, const sptrsv_schedule_t* s);
 int sptrsv_plan_get_schedule(sptrsv_plan_t plan, sptrsv_schedule_t* s);
+/* A partitioned plan's blocks (schedule with partitions >= 2): their count,
+ * the rows of the block system, the warm-up rows in all, the largest
+ * truncation bound (relative to max|x|, <= 2^-60) and, when table is not
+ * NULL, 4 ints per block: warm-up start s, first real row a, end e (the
+ * next block's a), first row in the block system. */
+int sptrsv_plan_partition_info(sptrsv_plan_t plan, int* blocks, int* n_ext, long long* warm_rows,
+                               double* bound, int* table);
 /* Re-reads gpu_L->a (same pattern) into the plan's value copies. */
 int sptrsv_plan_update_values(sptrsv_plan_t plan, const sp_mat_t* gpu_L);
 
@@ -332,6 +352,19 @@ int sptrsv_batch_set_schedule(sptrsv_batch_t batch, int mode, int block_warps, i
 int sptrsv_batch_set_seq_width(sptrsv_batch_t batch, double width);
 /* Systems solved sequentially, warps they occupy, rows left to the level tasks. */
 int sptrsv_batch_seq_systems(sptrsv_batch_t batch, int* nseq, int* nseq_warps, int* n_level_rows);
+/* Partitioned batch: every system of at least 2 * block_rows rows whose
+ * rows are all diagonally dominant is cut into about n_s / block_rows blocks
+ * solved independently after a warm-up (see sptrsv_schedule_t.partitions:
+ * each block starts early from a zero boundary, far enough that a proven
+ * bound on the dropped rows' effect is below 2^-60 relative to max|x|); the
+ * blocks and the other systems are solved as one batch of their own, b
+ * gathered into it and x scattered back inside every solve (and graph).
+ * block_rows: 0 (plain batch) or >= 256.  Keeps the schedule. */
+int sptrsv_batch_set_partition(sptrsv_batch_t batch, int block_rows);
+/* Systems cut into blocks, systems of the inner batch, warm-up rows in all,
+ * the largest truncation bound. */
+int sptrsv_batch_partition_info(sptrsv_batch_t batch, int* systems_cut, int* inner_systems, long long* warm_rows,
+                                double* bound);
 /* b, x: DEVICE packed vectors; precision 64 plain FP64, 32 FP32 + FP64 refinement. */
 int sptrsv_batch_solve(sptrsv_batch_t batch, const double* b, double* x, int precision, cudaStream_t stream);
 /* Same solve captured once as a CUDA graph for these (b, x, precision) and

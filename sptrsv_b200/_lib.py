@@ -27,7 +27,7 @@ SPTRSV_ERR_ALLOC = -7
 SPTRSV_ERR_NOT_CONVERGED = -8
 SPTRSV_ERR_UNSUPPORTED = -9
 
-VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER, VAR_STRIP, VAR_WAVE = 0, 1, 2, 3, 4, 5
+VAR_SIMPLE, VAR_ORDER, VAR_MULTIROW, VAR_CLUSTER, VAR_STRIP, VAR_WAVE, VAR_BAND = 0, 1, 2, 3, 4, 5, 6
 N_VARIANTS = 6
 
 
@@ -59,7 +59,8 @@ class Schedule(ctypes.Structure):
     """sptrsv_schedule_t."""
 
     _fields_ = [("variant", c_int), ("rows_per_warp", c_int), ("block_warps", c_int), ("warps_per_sm", c_int),
-                ("backoff_ns", c_int), ("ir_max_iters", c_int), ("band_levels", c_int), ("cluster_rows", c_int)]
+                ("backoff_ns", c_int), ("ir_max_iters", c_int), ("band_levels", c_int), ("cluster_rows", c_int),
+                ("partitions", c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -97,6 +98,8 @@ _SIGS = {
     "sptrsv_plan_set_schedule": (c_int, [c_void_p, POINTER(Schedule)]),
     "sptrsv_plan_get_schedule": (c_int, [c_void_p, POINTER(Schedule)]),
     "sptrsv_plan_update_values": (c_int, [c_void_p, POINTER(SpMat)]),
+    "sptrsv_plan_partition_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong),
+                                           POINTER(c_double), c_void_p]),
     "sptrsv_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_ir": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_solve_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
@@ -107,6 +110,9 @@ _SIGS = {
     "sptrsv_solve_ir_noalloc": (c_int, [POINTER(SpMat), c_void_p, c_void_p, c_int, c_void_p]),
     "sptrsv_batch_create": (c_int, [c_int, POINTER(SpMat), c_void_p, POINTER(c_void_p)]),
     "sptrsv_batch_destroy": (c_int, [c_void_p]),
+    "sptrsv_batch_set_partition": (c_int, [c_void_p, c_int]),
+    "sptrsv_batch_partition_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong),
+                                            POINTER(c_double)]),
     "sptrsv_batch_info": (c_int, [c_void_p, c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong)]),
     "sptrsv_batch_set_schedule": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int]),
     "sptrsv_batch_set_seq_width": (c_int, [c_void_p, c_double]),

@@ -35,6 +35,16 @@ class Batch:
         systems on one warp each, see set_seq_width)."""
         C.check(C.lib().sptrsv_batch_set_schedule(self._h, mode, block_warps, warps_per_sm, backoff_ns, ir_iters))
 
+    def set_partition(self, block_rows: int):
+        """Cut long diagonally dominant systems into blocks of about block_rows
+        rows solved independently after a warm-up (0: no cutting)."""
+        C.check(C.lib().sptrsv_batch_set_partition(self._h, int(block_rows)))
+
+    def partition_info(self) -> dict:
+        cut, inner, warm, bound = c_int(0), c_int(0), c_longlong(0), C.c_double(0)
+        C.check(C.lib().sptrsv_batch_partition_info(self._h, byref(cut), byref(inner), byref(warm), byref(bound)))
+        return {"systems_cut": cut.value, "inner_systems": inner.value, "warm_rows": warm.value, "bound": bound.value}
+
     def set_seq_width(self, width: float):
         C.check(C.lib().sptrsv_batch_set_seq_width(self._h, float(width)))
 

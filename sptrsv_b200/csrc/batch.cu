@@ -33,9 +33,14 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
+
+namespace sptrsv {
+constexpr long long kSegChunk = 8192;  // elements per copy chunk of a partitioned batch
+}
 
 
 struct sptrsv_batch_s {
@@ -94,6 +99,19 @@ struct sptrsv_batch_s {
     double seq_width = 16.0;     // mode 2: sequential when n_s / nlevs_s < seq_width
     int mode = 2;                // 0: level-ordered tasks, 1: natural-order chunks, 2: hybrid
     int block_warps = 8, warps_per_sm = 0, backoff_ns = 0, ir_iters = 2;
+    // partitioned batch (sptrsv_batch_set_partition): the block systems of the
+    // long systems and the other systems whole, as a batch of their own; b is
+    // gathered into its packed vectors and x scattered back, in chunks of at
+    // most kSegChunk elements (gather chunks first, then scatter chunks)
+    sptrsv_batch_s* inner = nullptr;
+    int part_rows = 0;
+    long long* d_seg = nullptr;  // [nseg * 3]: source offset, destination offset, length
+    int nseg_g = 0, nseg_s = 0;
+    double* pbx = nullptr;       // [inner->nvec] gathered right-hand sides
+    double* pxx = nullptr;       // [inner->nvec] block-system solutions
+    int part_systems = 0;        // systems cut into blocks
+    long long part_warm = 0;     // warm-up rows in all
+    double part_bound = 0;       // largest truncation bound of a block
     // graph cache for one (b, x, precision)
     cudaGraphExec_t gexec = nullptr;
     const double* g_b = nullptr;
@@ -715,8 +733,28 @@ __global__ void k_task_kp(const int* __restrict__ tbase, int ntasks, const int* 
         tkp[t] = 1 << (key_sorted[tbase[t]] % 6);
 }
 
+void batch_free(sptrsv_batch_s* B);
+
+void batch_part_free(sptrsv_batch_s* B)
+{
+    if (B->inner) {
+        batch_free(B->inner);
+        delete B->inner;
+        B->inner = nullptr;
+    }
+    cudaFree(B->d_seg); cudaFree(B->pbx); cudaFree(B->pxx);
+    B->d_seg = nullptr;
+    B->pbx = B->pxx = nullptr;
+    B->nseg_g = B->nseg_s = 0;
+    B->part_rows = 0;
+    B->part_systems = 0;
+    B->part_warm = 0;
+    B->part_bound = 0;
+}
+
 void batch_free(sptrsv_batch_s* B)
 {
+    batch_part_free(B);
     if (B->gexec) cudaGraphExecDestroy(B->gexec);
     if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
     cudaFree(B->nptr); cudaFree(B->ncol); cudaFree(B->nval64); cudaFree(B->nval32); cudaFree(B->ndg64);
@@ -987,9 +1025,29 @@ int batch_residual(sptrsv_batch_s* B, const double* b, const double* x, cudaStre
     return 0;
 }
 
+// Contiguous copies dst[d + t] = src[so + t], one block per table entry.
+__global__ void __launch_bounds__(256) k_seg_copy(const long long* __restrict__ seg, const double* __restrict__ src,
+                                                  double* __restrict__ dst)
+{
+    const long long* q = seg + 3 * (long long)blockIdx.x;
+    const long long so = q[0], d = q[1], len = q[2];
+    for (long long t = threadIdx.x; t < len; t += blockDim.x) dst[d + t] = src[so + t];
+}
+
 int batch_solve_impl(sptrsv_batch_s* B, const double* b, double* x, int precision, cudaStream_t s)
 {
     if (B->n == 0) return 0;
+    if (B->inner) {
+        // partitioned: every refinement step runs on the block systems, whose
+        // real rows equal the systems' rows to within the warm-up bound
+        if (B->nseg_g) k_seg_copy<<<B->nseg_g, 256, 0, s>>>(B->d_seg, b, B->pbx);
+        SPT_CUDA(cudaGetLastError());
+        int e = batch_solve_impl(B->inner, B->pbx, B->pxx, precision, s);
+        if (e) return e;
+        if (B->nseg_s) k_seg_copy<<<B->nseg_s, 256, 0, s>>>(B->d_seg + 3LL * B->nseg_g, B->pxx, x);
+        SPT_CUDA(cudaGetLastError());
+        return 0;
+    }
     if (precision == 64) {
         SPT_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(double) * (size_t)B->nvec, s));
         return batch_launch<double, double, double, 0>(B, false, b, x, nullptr, s);
@@ -1290,6 +1348,7 @@ int sptrsv_batch_set_schedule(sptrsv_batch_t B, int mode, int block_warps, int w
         B->gexec = nullptr;
     }
     int e = batch_apply_schedule(B, 0);
+    if (!e && B->inner) e = sptrsv_batch_set_schedule(B->inner, mode, block_warps, warps_per_sm, backoff_ns, ir_iters);
     return e ? e : ok();
 }
 
@@ -1302,12 +1361,14 @@ int sptrsv_batch_set_seq_width(sptrsv_batch_t B, double width)
         B->gexec = nullptr;
     }
     int e = batch_apply_schedule(B, 0);
+    if (!e && B->inner) e = sptrsv_batch_set_seq_width(B->inner, width);
     return e ? e : ok();
 }
 
 int sptrsv_batch_seq_systems(sptrsv_batch_t B, int* nseq, int* nseq_warps, int* n_level_rows)
 {
     if (!B) return set_error(SPTRSV_ERR_INVALID_ARG, "batch_seq_systems: NULL");
+    if (B->inner) B = B->inner;  // a partitioned batch runs its block systems
     int c = 0;
     for (char f : B->seq) c += f ? 1 : 0;
     if (nseq) *nseq = c;
@@ -1359,6 +1420,177 @@ int sptrsv_batch_solve_graph(sptrsv_batch_t B, const double* b, double* x, int p
         B->g_prec = precision;
     }
     SPT_CUDA(cudaGraphLaunch(B->gexec, s));
+    return ok();
+}
+
+}  // extern "C"
+
+namespace sptrsv {
+int partition_blocks(const int* rp, const int* ci, const double* va, int n, int P, int threads, std::vector<int>& tab,
+                     int* reach, double* bound);
+}
+
+extern "C" {
+
+// Cuts every system of at least 2 * block_rows rows (and whose rows are all
+// diagonally dominant) into about n_s / block_rows blocks with warm-ups (the
+// partitioned solve of the plan API: each block starts early from a zero
+// boundary, the start chosen so that a proven bound on the dropped rows'
+// effect is below 2^-60 relative to max|x|), and solves all blocks and the
+// other systems as one batch.  block_rows = 0 returns to the plain batch.
+int sptrsv_batch_set_partition(sptrsv_batch_t B, int block_rows)
+{
+    if (!B || block_rows < 0 || (block_rows > 0 && block_rows < 256))
+        return set_error(SPTRSV_ERR_INVALID_ARG, "batch_set_partition: block_rows must be 0 or >= 256");
+    if (B->gexec) {
+        cudaGraphExecDestroy(B->gexec);
+        B->gexec = nullptr;
+    }
+    if (block_rows == B->part_rows) return ok();
+    batch_part_free(B);
+    if (block_rows == 0) return ok();
+    const int n = B->n, m = B->m, nsys = B->nsys;
+    std::vector<int> nptr(n + 1), ncol(m > 0 ? m : 1);
+    std::vector<double> nval(m > 0 ? m : 1), ndg(n);
+    SPT_CUDA(cudaMemcpy(nptr.data(), B->nptr, sizeof(int) * (size_t)(n + 1), cudaMemcpyDeviceToHost));
+    if (m > 0) {
+        SPT_CUDA(cudaMemcpy(ncol.data(), B->ncol, sizeof(int) * (size_t)m, cudaMemcpyDeviceToHost));
+        SPT_CUDA(cudaMemcpy(nval.data(), B->nval64, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost));
+    }
+    SPT_CUDA(cudaMemcpy(ndg.data(), B->ndg64, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+    // per system: its blocks (s, a, e) in local rows; one block [0, 0, n_s) when not cut
+    std::vector<std::vector<int>> tabs(nsys);
+    std::vector<double> bounds(nsys, 0.0);
+    {
+        const int nt = std::max(1u, std::thread::hardware_concurrency());
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; t++)
+            th.emplace_back([&, t]() {
+                std::vector<int> rp, ci;
+                std::vector<double> va;
+                for (int sy = t; sy < nsys; sy += nt) {
+                    const int r0 = B->row0h[sy], ns = B->row0h[sy + 1] - r0;
+                    const int P = std::min(4096, ns / block_rows);
+                    tabs[sy] = {0, 0, ns, 0};
+                    if (P < 2) continue;
+                    rp.assign(ns + 1, 0);
+                    ci.clear();
+                    va.clear();
+                    for (int r = 0; r < ns; r++) {
+                        for (int q = nptr[r0 + r]; q < nptr[r0 + r + 1]; q++) {
+                            ci.push_back(ncol[q] - r0);
+                            va.push_back(nval[q]);
+                        }
+                        ci.push_back(r);
+                        va.push_back(ndg[r0 + r]);
+                        rp[r + 1] = (int)ci.size();
+                    }
+                    std::vector<int> tab;
+                    int w = 0;
+                    double bnd = 0;
+                    if (partition_blocks(rp.data(), ci.data(), va.data(), ns, P, 1, tab, &w, &bnd) == 0) {
+                        tabs[sy] = tab;
+                        bounds[sy] = bnd;
+                    }
+                }
+            });
+        for (auto& x : th) x.join();
+    }
+    // the block systems as device CSRs, and the copy tables
+    std::vector<sp_mat_t> mats;
+    std::vector<int> ks;
+    std::vector<long long> gseg, sseg;
+    auto add_chunks = [](std::vector<long long>& v, long long so, long long d, long long len) {
+        for (long long o = 0; o < len; o += kSegChunk) {
+            v.push_back(so + o);
+            v.push_back(d + o);
+            v.push_back(std::min<long long>(kSegChunk, len - o));
+        }
+    };
+    auto free_mats = [&]() {
+        for (auto& mm : mats) free_device_analysis(&mm, nullptr);
+    };
+    long long ioff = 0;
+    int cut = 0;
+    long long warm = 0;
+    double bound = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> va;
+    for (int sy = 0; sy < nsys; sy++) {
+        const int r0 = B->row0h[sy];
+        const int k = B->kk[sy];
+        const std::vector<int>& tab = tabs[sy];
+        const int P = (int)tab.size() / 4;
+        if (P > 1) {
+            cut++;
+            bound = std::max(bound, bounds[sy]);
+        }
+        for (int i = 0; i < P; i++) {
+            const int s0 = tab[4 * i], a = tab[4 * i + 1], e = tab[4 * i + 2];
+            warm += a - s0;
+            rp.assign(e - s0 + 1, 0);
+            ci.clear();
+            va.clear();
+            for (int r = s0; r < e; r++) {
+                for (int q = nptr[r0 + r]; q < nptr[r0 + r + 1]; q++)
+                    if (ncol[q] - r0 >= s0) {
+                        ci.push_back(ncol[q] - r0 - s0);
+                        va.push_back(nval[q]);
+                    }
+                ci.push_back(r - s0);
+                va.push_back(ndg[r0 + r]);
+                rp[r - s0 + 1] = (int)ci.size();
+            }
+            sp_mat_t mm{};
+            int err = allocate_memory(rp.data(), ci.data(), va.data(), e - s0, &mm, ALL);
+            if (err) {
+                free_mats();
+                return err;
+            }
+            mats.push_back(mm);
+            ks.push_back(k);
+            add_chunks(gseg, B->off[sy] + (long long)s0 * k, ioff, (long long)(e - s0) * k);
+            add_chunks(sseg, ioff + (long long)(a - s0) * k, B->off[sy] + (long long)a * k, (long long)(e - a) * k);
+            ioff += (long long)(e - s0) * k;
+        }
+    }
+    sptrsv_batch_t in = nullptr;
+    int err = sptrsv_batch_create((int)mats.size(), mats.data(), ks.data(), &in);
+    free_mats();
+    if (err) return err;
+    B->inner = in;
+    auto fail = [&](int code) {
+        batch_part_free(B);
+        return code;
+    };
+    err = sptrsv_batch_set_seq_width(in, B->seq_width);
+    if (!err) err = sptrsv_batch_set_schedule(in, B->mode, B->block_warps, B->warps_per_sm, B->backoff_ns, B->ir_iters);
+    if (err) return fail(err);
+    if (gseg.size() / 3 > 0x7fffffffULL || sseg.size() / 3 > 0x7fffffffULL)
+        return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "batch_set_partition: too many copy chunks"));
+    B->nseg_g = (int)(gseg.size() / 3);
+    B->nseg_s = (int)(sseg.size() / 3);
+    gseg.insert(gseg.end(), sseg.begin(), sseg.end());
+    if (cudaMalloc((void**)&B->d_seg, sizeof(long long) * std::max<size_t>(1, gseg.size())) != cudaSuccess ||
+        cudaMemcpy(B->d_seg, gseg.data(), sizeof(long long) * gseg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc((void**)&B->pbx, sizeof(double) * (size_t)in->nvec) != cudaSuccess ||
+        cudaMalloc((void**)&B->pxx, sizeof(double) * (size_t)in->nvec) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "batch_set_partition: buffers"));
+    B->part_rows = block_rows;
+    B->part_systems = cut;
+    B->part_warm = warm;
+    B->part_bound = bound;
+    return ok();
+}
+
+int sptrsv_batch_partition_info(sptrsv_batch_t B, int* systems_cut, int* inner_systems, long long* warm_rows,
+                                double* bound)
+{
+    if (!B) return set_error(SPTRSV_ERR_INVALID_ARG, "batch_partition_info: NULL");
+    if (systems_cut) *systems_cut = B->inner ? B->part_systems : 0;
+    if (inner_systems) *inner_systems = B->inner ? B->inner->nsys : B->nsys;
+    if (warm_rows) *warm_rows = B->inner ? B->part_warm : 0;
+    if (bound) *bound = B->inner ? B->part_bound : 0.0;
     return ok();
 }
 

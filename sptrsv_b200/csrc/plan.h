@@ -19,6 +19,8 @@
 // hb/hx (n x nrhs f64) staging for the host-buffer entry point.
 #pragma once
 
+#include <vector>
+
 #include "sptrsv_b200.h"
 
 struct SptLayout {
@@ -67,6 +69,7 @@ struct WaveLayout {
     int* runc = nullptr;       // [nruns+1] first chunk of each run
     int* grun = nullptr;       // [ngroups+1] first run of each group
     int* grow = nullptr;       // [ngroups+1] first row of each group
+    int* gseq = nullptr;       // [ngroups] processing order of the groups (null: natural order)
     int ngroups = 0, G = 0, cap = 0;  // cap: most rows in one group
     int maxe = 0;                      // most entries of one slot
 };
@@ -82,6 +85,45 @@ struct MrhsTable {
     void* pbuf = nullptr;   // [npslots * kp] partial sums (f64; f32 solves use the front half)
     int* pcnt = nullptr;    // [nsplit] piece counters, cleared before each launch
     int U = 0;              // elements per lane per wait round the table was cut for
+};
+
+// BAND schedule (built on demand, see band.cu): per unit (the whole matrix,
+// or each block of a block system) the steps of its levels as fixed-size
+// records, FP64 and FP32 copies.
+constexpr int kBandU = 4;  // entries per lane per step
+struct BandLayout {
+    int U = 0, R = 0;          // entries per lane per step; ring slots (slot R is a constant 0)
+    int nunits = 0, nsteps = 0;
+    int* ustep = nullptr;      // [nunits+1] first step of each unit
+    unsigned char* rec64 = nullptr;  // [nsteps * rb64]
+    unsigned char* rec32 = nullptr;  // [nsteps * rb32]
+    int rb64 = 0, rb32 = 0;
+    int* bidx = nullptr;       // [nsteps * 32] row whose b a lane's row takes (-1: none)
+};
+
+// Partitioned solve (built on demand, see part.cu): the rows are cut into P
+// blocks; block i covers the real rows [a_i, e_i) and starts its substitution
+// at s_i <= a_i from a zero boundary.  The blocks, with every entry that
+// points before their start dropped, form one block-diagonal system of
+// n_ext rows (block i at rows base_i ...) that a plan of its own (sub)
+// solves with any variant; b is gathered into it and x scattered out of it.
+struct PartPlan {
+    int P = 0;
+    int n_ext = 0;
+    long long nnz_ext = 0;
+    long long warm_rows = 0;      // sum of a_i - s_i
+    double bound = 0;             // largest truncation bound of a block (relative to max|x|)
+    int reach = 0;                // most rows between an entry's column and its row
+    std::vector<int> tab;         // [P * 4]: s_i, a_i, e_i, base_i
+    int* d_tab = nullptr;
+    sp_mat_t ext{};               // device CSR of the block system
+    dfr_analysis_info_t info{};   // its analysis
+    struct sptrsv_plan_s* sub = nullptr;
+    double* bx = nullptr;         // [n_ext * nrhs] gathered right-hand sides
+    double* xx = nullptr;         // [n_ext * nrhs] block-system solution
+    float* bx32 = nullptr;        // FP32 gathered residuals
+    float* xx32 = nullptr;        // FP32 block-system solutions
+    int cap_rhs = 0;
 };
 
 struct sptrsv_plan_s {
@@ -123,6 +165,15 @@ struct sptrsv_plan_s {
     double* hx = nullptr;
     int cap_host = 0;
     sptrsv_schedule_t sched{};
+    PartPlan* part = nullptr;    // partitioned solve (sched.partitions >= 2)
+    // set on a block system's plan: the first row of every block (WAVE
+    // groups never span two blocks, and the blocks' groups are interleaved)
+    std::vector<int> blk_starts;
+    // set on a block system's plan: the outer plan's block table (s, a, e,
+    // base per block), so BAND records can read b and write x in the outer
+    // plan's rows directly
+    std::vector<int> part_tab;
+    BandLayout band;             // BAND layout (built on demand)
 };
 
 namespace sptrsv {
@@ -145,4 +196,24 @@ void wave_free(WaveLayout& w);
 // Builds (or keeps) the multi-RHS task table for kp lanes per row.
 int build_mrhs_tasks(sptrsv_plan_s* p, int kp, int U);
 void mrhs_free(MrhsTable& t);
+// Builds (or keeps) p->band; SPTRSV_ERR_UNSUPPORTED when a row is too long,
+// levels are too wide for one warp, or the ring would not fit.
+int build_band_layout(sptrsv_plan_s* p);
+void band_free(BandLayout& t);
+// One BAND solve of the plan (see band.cu): b FP64 or FP32 (b_f32); FP64
+// (x double) or FP32 (x float, may be null; x64 per out_mode) arithmetic.
+int band_solve(sptrsv_plan_s* p, bool f32, const void* b, bool b_f32, void* x, double* x64, int out_mode,
+               cudaStream_t s);
+// Builds (or keeps) p->part for P blocks; SPTRSV_ERR_UNSUPPORTED when L is
+// not row diagonally dominant or too small to cut.
+int build_part(sptrsv_plan_s* p, int P);
+void part_free(sptrsv_plan_s* p);
+// Partitioned solves (p->sched.partitions >= 2, p->part built).
+int part_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s);
+// FP32 solve of the block system for rhs (FP64 or FP32, n x nrhs): out32 =
+// L^-1 rhs, and x64 = out32 (OUT_SET64), x64 += out32 (OUT_ADD64) or
+// nothing (OUT_X).
+template <typename BT>
+int part_solve32(sptrsv_plan_s* p, const BT* rhs, float* out32, double* x64, int out_mode, int nrhs,
+                 cudaStream_t s);
 }  // namespace sptrsv

@@ -174,6 +174,8 @@ void plan_free_arrays(sptrsv_plan_s* p)
     cudaFree(p->clu_key); cudaFree(p->clu_tasks); cudaFree(p->clu_ctask);
     cudaFree(p->w32a); cudaFree(p->w32b); cudaFree(p->hb); cudaFree(p->hx);
     cudaFree(p->bflag);
+    part_free(p);
+    band_free(p->band);
     if (p->epochs) cudaFreeHost(p->epochs);
     if (p->ev_start) cudaEventDestroy(p->ev_start);
     if (p->ev_copied) cudaEventDestroy(p->ev_copied);
@@ -254,6 +256,7 @@ sptrsv_schedule_t default_schedule()
     s.ir_max_iters = 2;
     s.band_levels = 64;
     s.cluster_rows = 4096;
+    s.partitions = 0;
     return s;
 }
 
@@ -296,6 +299,24 @@ int plan_fill_values(sptrsv_plan_s* p, const sp_mat_t* L, cudaStream_t s)
         int e = build_strip_layout(p, R);
         if (e) return e;
     }
+    if (p->band.rec64) {  // the band records
+        SPT_CUDA(cudaStreamSynchronize(s));
+        band_free(p->band);
+        int e = build_band_layout(p);
+        if (e) return e;
+    }
+    if (p->part) {  // the block system: its warm-ups depend on the values
+        const int P = p->part->P;
+        SPT_CUDA(cudaStreamSynchronize(s));
+        part_free(p);
+        int e = build_part(p, P);
+        if (!e && p->sched.partitions >= 2) {
+            sptrsv_schedule_t inner = p->sched;
+            inner.partitions = 0;
+            e = sptrsv_plan_set_schedule(p->part->sub, &inner);
+        }
+        if (e) return e;
+    }
     return 0;
 }
 
@@ -334,6 +355,8 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
             di = reinterpret_cast<const V*>(l.di64);
         }
     };
+    if (sc.variant == SPTRSV_VAR_BAND && nrhs == 1)
+        return band_solve(p, f32, b, sizeof(BT) == 4, x, x64, OUT, s);
     if (sc.variant == SPTRSV_VAR_CLUSTER && nrhs == 1) {
         int e = build_cluster_layout(p, sc.band_levels, sc.cluster_rows);
         if (!e) e = build_cluster_tasks(p, sc.rows_per_warp);
@@ -372,7 +395,7 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
                       f32 ? reinterpret_cast<const V*>(t.ev32) : reinterpret_cast<const V*>(t.ev64),
                       f32 ? reinterpret_cast<const V*>(t.lsub32) : reinterpret_cast<const V*>(t.lsub64),
                       f32 ? reinterpret_cast<const V*>(t.di32) : reinterpret_cast<const V*>(t.di64), nullptr},
-                     t.runc, t.grun, t.grow};
+                     t.runc, t.grun, t.grow, t.gseq};
         auto kern = p->launch_bflag
                         ? (t.maxe <= 2         ? k_sptrsv_wave<V, T, BT, OUT, 2, false, true>
                            : t.maxe <= kStripU ? k_sptrsv_wave<V, T, BT, OUT, kStripU, false, true>
@@ -467,25 +490,82 @@ int plan_residual(sptrsv_plan_s* p, const double* b, const double* x, float* r32
     return 0;
 }
 
+static bool partitioned(const sptrsv_plan_s* p) { return p->part && p->sched.partitions >= 2; }
+
+int part_ensure(PartPlan* q, int k);
+int part_gather64(PartPlan* q, const double* src, double* dst, int k, cudaStream_t s);
+int part_gather32(PartPlan* q, const float* src, float* dst, int k, cudaStream_t s);
+int part_scatter64(PartPlan* q, const double* src, double* dst, int k, cudaStream_t s);
+int part_scatter32(PartPlan* q, const float* src, float* out32, double* x64, int mode, int k, cudaStream_t s);
+
 int plan_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s)
 {
+    if (partitioned(p)) return part_solve_f64(p, b, x, nrhs, s);
     SPT_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(double) * (size_t)p->n * nrhs, s));
     return plan_launch<double, double, double, OUT_X>(p, false, b, x, nullptr, nrhs, s);
+}
+
+// Partitioned FP64 solve: b gathered into the block system, solved there,
+// each block's real rows scattered into x.
+int part_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s)
+{
+    PartPlan* q = p->part;
+    if (q->sub->sched.variant == SPTRSV_VAR_BAND && nrhs == 1)  // records map to this plan's rows
+        return band_solve(q->sub, false, b, false, x, nullptr, OUT_X, s);
+    int e = part_ensure(q, nrhs);
+    if (!e) e = part_gather64(q, b, q->bx, nrhs, s);
+    if (!e) e = plan_solve_f64(q->sub, q->bx, q->xx, nrhs, s);
+    if (!e) e = part_scatter64(q, q->xx, x, nrhs, s);
+    return e;
+}
+
+template <typename BT>
+int part_solve32(sptrsv_plan_s* p, const BT* rhs, float* out32, double* x64, int out_mode, int nrhs, cudaStream_t s)
+{
+    PartPlan* q = p->part;
+    if (q->sub->sched.variant == SPTRSV_VAR_BAND && nrhs == 1)
+        return band_solve(q->sub, true, rhs, sizeof(BT) == 4, out32, x64, out_mode, s);
+    int e = part_ensure(q, nrhs);
+    if (e) return e;
+    const BT* g;
+    if constexpr (sizeof(BT) == 8) {
+        e = part_gather64(q, rhs, q->bx, nrhs, s);
+        g = q->bx;
+    } else {
+        e = part_gather32(q, rhs, q->bx32, nrhs, s);
+        g = q->bx32;
+    }
+    if (e) return e;
+    SPT_CUDA(cudaMemsetAsync(q->xx32, 0xFF, sizeof(float) * (size_t)q->n_ext * nrhs, s));
+    e = plan_launch<float, float, BT, OUT_X>(q->sub, true, g, q->xx32, nullptr, nrhs, s);
+    if (e) return e;
+    return part_scatter32(q, q->xx32, out32, x64, out_mode, nrhs, s);
+}
+template int part_solve32<double>(sptrsv_plan_s*, const double*, float*, double*, int, int, cudaStream_t);
+template int part_solve32<float>(sptrsv_plan_s*, const float*, float*, double*, int, int, cudaStream_t);
+
+// FP32 solve of rhs into out32 (the readiness flags of the unpartitioned
+// kernels, so never null there) and, per out_mode, x64 = or += the result.
+template <typename BT>
+int solve32(sptrsv_plan_s* p, const BT* rhs, float* out32, double* x64, int out_mode, int nrhs, cudaStream_t s)
+{
+    if (partitioned(p)) return part_solve32<BT>(p, rhs, out32, x64, out_mode, nrhs, s);
+    SPT_CUDA(cudaMemsetAsync(out32, 0xFF, sizeof(float) * (size_t)p->n * nrhs, s));
+    if (out_mode == OUT_SET64) return plan_launch<float, float, BT, OUT_SET64>(p, true, rhs, out32, x64, nrhs, s);
+    if (out_mode == OUT_ADD64) return plan_launch<float, float, BT, OUT_ADD64>(p, true, rhs, out32, x64, nrhs, s);
+    return plan_launch<float, float, BT, OUT_X>(p, true, rhs, out32, nullptr, nrhs, s);
 }
 
 int plan_solve_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s)
 {
     int e = plan_ensure_work(p, nrhs);
     if (e) return e;
-    const size_t bytes32 = sizeof(float) * (size_t)p->n * nrhs;
-    SPT_CUDA(cudaMemsetAsync(p->w32a, 0xFF, bytes32, s));
-    e = plan_launch<float, float, double, OUT_SET64>(p, true, b, p->w32a, x, nrhs, s);
+    e = solve32<double>(p, b, p->w32a, x, OUT_SET64, nrhs, s);
     if (e) return e;
     for (int it = 0; it < p->sched.ir_max_iters; it++) {
         e = plan_residual(p, b, x, p->w32b, nullptr, nrhs, s);
         if (e) return e;
-        SPT_CUDA(cudaMemsetAsync(p->w32a, 0xFF, bytes32, s));
-        e = plan_launch<float, float, float, OUT_ADD64>(p, true, p->w32b, p->w32a, x, nrhs, s);
+        e = solve32<float>(p, p->w32b, p->w32a, x, OUT_ADD64, nrhs, s);
         if (e) return e;
     }
     return 0;
@@ -523,7 +603,6 @@ int plan_calibrate_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, do
     int e = plan_ensure_work(p, nrhs);
     if (e) return e;
     const long long m = (long long)p->n * nrhs;
-    const size_t bytes32 = sizeof(float) * (size_t)m;
     unsigned long long* d_n = nullptr;  // [0] |x| (f64 bits), [1] |d| (f32 bits)
     SPT_CUDA(cudaMalloc((void**)&d_n, 2 * sizeof(unsigned long long)));
     cudaStream_t s = 0;
@@ -531,16 +610,14 @@ int plan_calibrate_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, do
         cudaFree(d_n);
         return code;
     };
-    if (cudaMemsetAsync(p->w32a, 0xFF, bytes32, s) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "calibrate"));
-    e = plan_launch<float, float, double, OUT_SET64>(p, true, b, p->w32a, x, nrhs, s);
+    e = solve32<double>(p, b, p->w32a, x, OUT_SET64, nrhs, s);
     if (e) return fail(e);
     int need = max_iters;
     double ratio = 0;
     for (int it = 1; it <= max_iters + 1; it++) {
         e = plan_residual(p, b, x, p->w32b, nullptr, nrhs, s);
         if (e) return fail(e);
-        cudaMemsetAsync(p->w32a, 0xFF, bytes32, s);
-        e = plan_launch<float, float, float, OUT_X>(p, true, p->w32b, p->w32a, nullptr, nrhs, s);
+        e = solve32<float>(p, p->w32b, p->w32a, nullptr, OUT_X, nrhs, s);
         if (e) return fail(e);
         cudaMemsetAsync(d_n, 0, 2 * sizeof(unsigned long long), s);
         k_absmax64<<<grid_for(m, 256), 256, 0, s>>>(x, m, d_n);
@@ -560,8 +637,7 @@ int plan_calibrate_ir(sptrsv_plan_s* p, const double* b, double* x, int nrhs, do
         }
         if (it == max_iters + 1) break;
         // apply the correction: x += d (the plain solve above wrote d to w32a only)
-        cudaMemsetAsync(p->w32a, 0xFF, bytes32, s);
-        e = plan_launch<float, float, float, OUT_ADD64>(p, true, p->w32b, p->w32a, x, nrhs, s);
+        e = solve32<float>(p, p->w32b, p->w32a, x, OUT_ADD64, nrhs, s);
         if (e) return fail(e);
     }
     cudaFree(d_n);
@@ -580,6 +656,8 @@ int check_schedule(const sptrsv_schedule_t* s)
     if (s->warps_per_sm < 0 || s->warps_per_sm > 64) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: warps_per_sm");
     if (s->backoff_ns < 0 || s->backoff_ns > 100000) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: backoff_ns");
     if (s->ir_max_iters < 0 || s->ir_max_iters > 16) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: ir_max_iters");
+    if (s->partitions < 0 || s->partitions > 4096)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: partitions must be in [0, 4096]");
     if (s->band_levels < 1 || s->band_levels > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: band_levels");
     if (s->cluster_rows < 32 || s->cluster_rows > 8192)
         return set_error(SPTRSV_ERR_INVALID_ARG, "schedule: cluster_rows must be in [32, 8192]");
@@ -690,7 +768,15 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
     if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: NULL argument");
     int e = check_schedule(s);
     if (e) return e;
-    if (s->variant == SPTRSV_VAR_CLUSTER) {
+    if (s->partitions >= 2) {
+        // the variant runs on the block system
+        e = build_part(p, s->partitions);
+        if (e) return e;
+        sptrsv_schedule_t inner = *s;
+        inner.partitions = 0;
+        e = sptrsv_plan_set_schedule(p->part->sub, &inner);
+        if (e) return e;
+    } else if (s->variant == SPTRSV_VAR_CLUSTER) {
         e = build_cluster_layout(p, s->band_levels, s->cluster_rows);
         if (!e) e = build_cluster_tasks(p, s->rows_per_warp);
         if (e) return e;
@@ -702,6 +788,9 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
         if (e) return e;
     } else if (s->variant == SPTRSV_VAR_WAVE) {
         e = build_wave_layout(p, s->block_warps, kWaveMaxRows);
+        if (e) return e;
+    } else if (s->variant == SPTRSV_VAR_BAND) {
+        e = build_band_layout(p);
         if (e) return e;
     }
     p->sched = *s;
@@ -745,8 +834,7 @@ int sptrsv_solve_f32(sptrsv_plan_t p, const double* b, float* x32, int nrhs, cud
 {
     if (!p || !b || !x32 || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f32: bad arguments");
     if (p->n == 0) return ok();
-    SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)p->n * nrhs, stream));
-    int e = plan_launch<float, float, double, OUT_X>(p, true, b, x32, nullptr, nrhs, stream);
+    int e = solve32<double>(p, b, x32, nullptr, OUT_X, nrhs, stream);
     return e ? e : ok();
 }
 
@@ -799,7 +887,7 @@ int sptrsv_solve_host(sptrsv_plan_t p, const double* hb, double* hx, int nrhs, i
         p->cap_host = nrhs;
     }
     void* hx_dev = nullptr;
-    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && mapped_host(hb) &&
+    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && !partitioned(p) && mapped_host(hb) &&
         (hx_dev = mapped_host(hx)) != nullptr) {
         int e = build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
         if (!e) e = solve_host_streamed(p, hb, (double*)hx_dev, s);

@@ -693,7 +693,8 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_strip(StripMat<V> m, int nstr
     }
 }
 
-// WAVE schedule (see strip.cu): CTA c takes line groups c, c + gridDim, ...;
+// WAVE schedule (see strip.cu): CTA c takes the groups at places c,
+// c + gridDim, ... of the processing order (gseq; natural order when null);
 // warp w of the CTA solves line w of the group chunk by chunk (the same
 // chunk arithmetic as STRIP).  The group's x values live in shared memory
 // (filled with the sentinel first): a column inside the group is encoded
@@ -724,6 +725,7 @@ struct WaveMat {
     const int* __restrict__ runc;  // first chunk of each run
     const int* __restrict__ grun;  // first run of each group
     const int* __restrict__ grow;  // first row of each group
+    const int* __restrict__ gseq;  // processing order of the groups (null: natural)
 };
 
 template <typename V, typename T, typename BT, int OUT, int U, bool MULTI, bool STREAM>
@@ -749,7 +751,8 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
         if (need) seg_ok = sg;
         return true;
     };
-    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    for (int k = blockIdx.x; k < ngroups; k += gridDim.x) {
+        const int g = w.gseq ? __ldg(w.gseq + k) : k;
         const int r0 = __ldg(w.grow + g), nr = __ldg(w.grow + g + 1) - r0;
         for (int t = threadIdx.x; t < nr; t += blockDim.x) xs[t] = sentinel_value<T>();
         __syncthreads();

@@ -187,6 +187,7 @@ void wave_free(WaveLayout& w)
 {
     cudaFree(w.row); cudaFree(w.pe); cudaFree(w.ecol); cudaFree(w.ev64); cudaFree(w.ev32); cudaFree(w.lsub64);
     cudaFree(w.lsub32); cudaFree(w.di64); cudaFree(w.di32); cudaFree(w.runc); cudaFree(w.grun); cudaFree(w.grow);
+    cudaFree(w.gseq);
     w = WaveLayout{};
 }
 
@@ -440,19 +441,51 @@ int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows)
         cudaError_t e_ = (call);                                  \
         if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
     } while (0)
-    // runs (grid lines) and groups of G runs
+    // runs (grid lines) and groups of G runs; on a block system (blk_starts
+    // set) a group also ends before a run that starts a block
     std::vector<int> run0;
     for (int q = 0; q < nch; q++)
         if (q == 0 || !ch.linked[q]) run0.push_back(q);
     const int nruns = (int)run0.size();
     run0.push_back(nch);
-    const int ngroups = (nruns + G - 1) / G;
-    std::vector<int> grun(ngroups + 1), grow(ngroups + 1), g0(nch), ident(nch);
+    std::vector<int> grun, blk_of_group;
+    {
+        size_t nb = 0;  // blocks whose start is at or before the current run
+        int in_group = 0;
+        for (int r = 0; r < nruns; r++) {
+            const int row = ch.cstart[run0[r]];
+            bool starts_block = false;
+            while (nb < p->blk_starts.size() && p->blk_starts[nb] <= row) {
+                starts_block = p->blk_starts[nb] == row;
+                nb++;
+            }
+            if (r == 0 || in_group == G || starts_block) {
+                grun.push_back(r);
+                blk_of_group.push_back(nb > 0 ? (int)nb - 1 : 0);
+                in_group = 0;
+            }
+            in_group++;
+        }
+        grun.push_back(nruns);
+    }
+    const int ngroups = (int)grun.size() - 1;
+    std::vector<int> grow(ngroups + 1), g0(nch), ident(nch);
     int cap = 0;
     for (int g = 0; g <= ngroups; g++) {
-        grun[g] = std::min(nruns, g * G);
         grow[g] = ch.cstart[run0[grun[g]]];
         if (g > 0) cap = std::max(cap, grow[g] - grow[g - 1]);
+    }
+    // processing order: natural, or on a block system the blocks' groups
+    // interleaved (the j-th group of every block, then the (j+1)-th), which is
+    // topological because a group depends only on groups of its own block
+    std::vector<int> gseq;
+    if (!p->blk_starts.empty() && ngroups > 0) {
+        std::vector<int> rank(ngroups);
+        for (int g = 0; g < ngroups; g++)
+            rank[g] = (g > 0 && blk_of_group[g] == blk_of_group[g - 1]) ? rank[g - 1] + 1 : 0;
+        gseq.resize(ngroups);
+        for (int g = 0; g < ngroups; g++) gseq[g] = g;
+        std::stable_sort(gseq.begin(), gseq.end(), [&](int a, int b) { return rank[a] < rank[b]; });
     }
     if (cap > max_rows)
         return fail(set_error(SPTRSV_ERR_UNSUPPORTED, "wave schedule: %d lines of the matrix hold %d rows, more than "
@@ -468,6 +501,10 @@ int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows)
     WCHK(cudaMemcpy(w.runc, run0.data(), sizeof(int) * (size_t)(nruns + 1), cudaMemcpyHostToDevice));
     WCHK(cudaMemcpy(w.grun, grun.data(), sizeof(int) * (size_t)(ngroups + 1), cudaMemcpyHostToDevice));
     WCHK(cudaMemcpy(w.grow, grow.data(), sizeof(int) * (size_t)(ngroups + 1), cudaMemcpyHostToDevice));
+    if (!gseq.empty()) {
+        WCHK(dalloc(&w.gseq, ngroups));
+        WCHK(cudaMemcpy(w.gseq, gseq.data(), sizeof(int) * (size_t)ngroups, cudaMemcpyHostToDevice));
+    }
     WCHK(cudaMemcpy(d_ident, ident.data(), sizeof(int) * (size_t)nch, cudaMemcpyHostToDevice));
     WCHK(cudaMemcpy(d_g0, g0.data(), sizeof(int) * (size_t)nch, cudaMemcpyHostToDevice));
     // slots and entries in natural chunk order

@@ -52,6 +52,7 @@ int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
     s->ir_max_iters = 2;
     s->band_levels = 64;
     s->cluster_rows = 4096;
+    s->partitions = 0;
     if (v == SPTRSV_VAR_SIMPLE && nat_v[j] != SPTRSV_VAR_SIMPLE) {
         s->variant = nat_v[j];
         s->rows_per_warp = 1;

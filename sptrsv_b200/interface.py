@@ -183,9 +183,10 @@ class Plan:
         return self._h
 
     def set_schedule(self, variant: int, rows_per_warp: int = 1, ir_max_iters: int = 2, block_warps: int = 8,
-                     warps_per_sm: int = 0, backoff_ns: int = 0, band_levels: int = 64, cluster_rows: int = 4096):
+                     warps_per_sm: int = 0, backoff_ns: int = 0, band_levels: int = 64, cluster_rows: int = 4096,
+                     partitions: int = 0):
         s = Schedule(variant, rows_per_warp, block_warps, warps_per_sm, backoff_ns, ir_max_iters, band_levels,
-                     cluster_rows)
+                     cluster_rows, partitions)
         C.check(C.lib().sptrsv_plan_set_schedule(self._h, byref(s)))
 
     def set_schedule_struct(self, s: Schedule):
@@ -198,6 +199,16 @@ class Plan:
 
     def update_values(self, gpu_L: SpMat):
         C.check(C.lib().sptrsv_plan_update_values(self._h, byref(gpu_L)))
+
+    def partition_info(self) -> dict:
+        """Blocks of a partitioned schedule: count, block-system rows, warm-up
+        rows, truncation bound and the (s, a, e, base) table per block."""
+        nb, ne, wr, bd = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        C.check(C.lib().sptrsv_plan_partition_info(self._h, byref(nb), byref(ne), byref(wr), byref(bd), None))
+        tab = np.zeros(4 * nb.value, dtype=np.int32)
+        C.check(C.lib().sptrsv_plan_partition_info(self._h, None, None, None, None, tab.ctypes.data))
+        return {"blocks": nb.value, "n_ext": ne.value, "warm_rows": wr.value, "bound": bd.value,
+                "table": tab.reshape(-1, 4)}
 
     def solve_f64(self, b, x, nrhs: int = 1, stream=None):
         m = self.n * nrhs

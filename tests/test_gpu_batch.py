@@ -170,3 +170,97 @@ def test_batch_long_chains_one_warp_per_rhs(torch_cuda, precision):
     batch.close()
     for d in dev:
         S.free_device_analysis(d, None)
+
+
+def test_full_c3_batch_fp64_and_ir_graph(torch_cuda):
+    """The full batched configuration: 512 banded systems, n log-uniform in
+    [1e3, 2e5], bandwidth log-uniform in [16, 4096], 4-16 off-diagonals per
+    row, 1-32 right-hand sides each (2.4e9-byte packed vectors, int64
+    packed offsets).  FP64 and FP32 + FP64 refinement through the CUDA
+    graph, replayed twice, every system against the oracle; then the hybrid
+    split with more systems on sequential warps, where systems with many
+    right-hand sides are cut into one unit per column."""
+    import sptrsv_b200 as S
+    from sptrsv_b200.batch import Batch
+
+    torch = torch_cuda
+    mats, ks, xs = gen.batch_config(512, seed=3)
+    dev = [S.allocate_memory(m.rowptr, m.colidx, m.val, m.n) for m in mats]
+    bs = [m.matvec(x, k) for m, x, k in zip(mats, xs, ks)]
+    batch = Batch(dev, ks)
+    assert batch.vec_len == sum(m.n * k for m, k in zip(mats, ks)) and batch.vec_len > 2**31
+    refs = [O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k) for m, b, k in zip(mats, bs, ks)]  # about 2 s
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    del bs
+    dx = torch.empty_like(db)
+
+    def check(tag):
+        xh = dx.cpu().numpy()
+        worst = 0.0
+        for s in range(len(mats)):
+            a, b = batch.offsets[s], batch.offsets[s + 1]
+            worst = max(worst, O.rel_err(xh[a:b], refs[s]))
+        assert worst <= TOL, (tag, worst)
+        return worst
+
+    for part, sched, width, prec, iters in ((0, dict(mode=2, block_warps=4), 16.0, 64, 0),
+                                            (0, dict(mode=2, block_warps=4), 16.0, 32, 1),
+                                            (0, dict(mode=2, block_warps=8), 64.0, 64, 0),
+                                            (4096, dict(mode=2, block_warps=4), 16.0, 64, 0),
+                                            (4096, dict(mode=2, block_warps=4), 16.0, 32, 1)):
+        batch.set_partition(part)
+        batch.set_seq_width(width)
+        batch.set_schedule(ir_iters=iters, **sched)
+        for rep in range(2):
+            dx.fill_(0)
+            batch.solve_graph(db, dx, prec)
+            S.sync_status()
+            check((sched, width, prec, rep))
+    nseq, nseqw, _ = batch.seq_systems()
+    assert nseq > 0 and nseqw >= nseq
+    batch.close()
+    for d in dev:
+        S.free_device_analysis(d, None)
+
+
+@pytest.mark.parametrize("block_rows", [256, 1500])
+def test_batch_partitioned(torch_cuda, block_rows):
+    """Long systems cut into blocks with warm-ups, solved as a batch of block
+    systems; FP64 and FP32 + refinement, plain and graph solves, against the
+    oracle; then back to the plain batch."""
+    import sptrsv_b200 as S
+    from sptrsv_b200.batch import Batch
+
+    torch = torch_cuda
+    mats, ks, xs, dev, bs, refs = _make(S, 40, seed=17, n_hi=20000)
+    batch = Batch(dev, ks)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.empty_like(db)
+    batch.set_partition(block_rows)
+    pi = batch.partition_info()
+    long_sys = sum(1 for m in mats if m.n >= 2 * block_rows)
+    assert 0 < pi["systems_cut"] <= long_sys and pi["inner_systems"] > len(mats)
+    assert pi["warm_rows"] > 0 and 0.0 <= pi["bound"] <= 2.0 ** -60
+    for sched, width in ((dict(mode=2, block_warps=4), 16.0), (dict(mode=0), 16.0), (dict(mode=2), 1e9)):
+        batch.set_seq_width(width)
+        for prec, iters in ((64, 0), (32, 2)):
+            batch.set_schedule(ir_iters=iters, **sched)
+            for solve in (batch.solve, batch.solve_graph):
+                dx.fill_(0)
+                solve(db, dx, prec)
+                S.sync_status()
+                xh = dx.cpu().numpy()
+                for s in range(len(mats)):
+                    a, b = batch.offsets[s], batch.offsets[s + 1]
+                    assert O.rel_err(xh[a:b], refs[s]) <= TOL, (s, sched, prec)
+    batch.set_partition(0)
+    assert batch.partition_info()["systems_cut"] == 0
+    batch.solve(db, dx, 64)
+    S.sync_status()
+    xh = dx.cpu().numpy()
+    for s in range(len(mats)):
+        a, b = batch.offsets[s], batch.offsets[s + 1]
+        assert O.rel_err(xh[a:b], refs[s]) <= TOL
+    batch.close()
+    for d in dev:
+        S.free_device_analysis(d, None)
