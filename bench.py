@@ -73,6 +73,25 @@ def f32_launch_bytes(n: int, nnz: int, k: int) -> int:
     return 4 * (n + 1) + 4 * n + 4 * n + 8 * (nnz - n) + 8 * n * k + 4 * n * k
 
 
+def solve_launches(sched, mode: int, ir_iters: int) -> int:
+    """Kernels of the library launched per solve: the solve kernel, plus a
+    gather of b into the block system and a scatter of x out of it when
+    partitioned (BAND writes x itself), plus b into BAND's records; FP32 +
+    refinement adds a residual and another solve per step."""
+    band = sched.variant == 6
+    part = sched.partitions >= 2
+    one = 2 if band else (3 if part else 1)
+    return one if mode == 64 else one * (1 + ir_iters) + ir_iters
+
+
+def selector_ready(SEL) -> bool:
+    """Trained weights for the library's current class table are present."""
+    if not SELECTOR_WEIGHTS.exists():
+        return False
+    z = np.load(SELECTOR_WEIGHTS)
+    return (int(z["table"]) if "table" in z.files else 1) == SEL.CLASS_TABLE
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -475,7 +494,7 @@ def run_ours(args, rank, world, local, dist):
 
     if args.lean:
         # profiling run: one fixed schedule, warm-up and the timed steps, nothing else
-        cls = args.fixed_class if args.fixed_class >= 0 else 3  # wave/G8
+        cls = args.fixed_class if args.fixed_class >= 0 else 4  # wave/G4 over 16 blocks
         s = SEL.schedule_from_class(cls)
         s.ir_max_iters = 1
         plan.set_schedule_struct(s)
@@ -496,7 +515,7 @@ def run_ours(args, rank, world, local, dist):
     learned = None
     if args.fixed_class >= 0:
         cls64 = cls32 = args.fixed_class
-    elif SELECTOR_WEIGHTS.exists():
+    elif selector_ready(SEL):
         net = SEL.Mlp.load(SELECTOR_WEIGHTS)
         c = net.select(plan, L, info)  # best predicted class that applies to this matrix
         learned = {"class": c, "name": SEL.class_name(c), "time_over_best_fp64": float(times64[c] / times64[cls64])}
@@ -542,7 +561,7 @@ def run_ours(args, rank, world, local, dist):
     total_ms = reduce_max(dist, sum(ts))
     value = world * k * args.steps / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
-    launches_per_step = 1 if mode == 64 else 1 + 2 * ir_iters
+    launches_per_step = solve_launches(SEL.schedule_from_class(sel64 if mode == 64 else sel32), mode, ir_iters)
 
     # --- the other mode and the drop-in FP64 path
     other = 32 if mode == 64 else 64
@@ -572,7 +591,8 @@ def run_ours(args, rank, world, local, dist):
     sched = SEL.schedule_from_class(sel64 if mode == 64 else sel32)
     variant = SEL.VARIANT_NAMES[sched.variant]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": load_traffic(f"{variant}_{'f64' if mode == 64 else 'f32'}_{args.config}"),
+                "traffic": load_traffic(f"{variant}{f'_p{sched.partitions}' if sched.partitions >= 2 else ''}"
+                                        f"_{'f64' if mode == 64 else 'f32'}_{args.config}"),
                 "kernel": kname, "algorithmic_bytes_per_launch": bytes_kern, "launch_ms": t_kern,
                 "peak_kind": peak_kind}
     if not args.extra:
@@ -808,7 +828,8 @@ def run_batch(args, rank, world, local, dist):
         "e2e": {"value": world * nk / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 8 * batch.vec_len,
                 "d2h_bytes_per_step": 8 * batch.vec_len},
         "energy_j_per_solve": energy.get("j_per_solve"), "energy": energy,
-        "roofline": roofline, "gpu_launches": args.steps * (1 if prec == 64 else 1 + 2 * iters),
+        "roofline": roofline,
+        "gpu_launches": args.steps * ((1 if prec == 64 else 1 + 2 * iters) + (2 if part else 0)),
         "clocks": clocks, "cpu_baseline": cpu,
     }
     batch.close()

@@ -234,8 +234,8 @@ typedef struct {
                           /* zero boundary (its warm-up), K_i chosen at plan time so  */
                           /* that a proven bound on the effect of the dropped rows is */
                           /* below 2^-60 relative to max|x|.  Needs a row diagonally  */
-                          /* dominant L (|L_ii| >= sum_j |L_ij|), else                */
-                          /* SPTRSV_ERR_UNSUPPORTED.  P <= 4096.                      */
+                          /* dominant L (|L_ii| >= sum_j |L_ij|) and at least 256     */
+                          /* rows per block, else SPTRSV_ERR_UNSUPPORTED.  P <= 4096. */
 } sptrsv_schedule_t;
 
 /* Creates a plan for the analysed matrix.  info must come from run_analysis

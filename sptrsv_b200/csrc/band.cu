@@ -14,20 +14,18 @@
 //
 // Records.  A unit's levels are cut into steps of at most 32/kp rows with
 // kp lanes per row (the smallest power of two that gives every row of the
-// level at most U entries per lane); step t is one fixed-size record:
-//   int   hdr[4]          kp, level_end (1 on a level's last step), 0, 0
-//   T     val[U][32]      entry u of lane j (0 for an unused entry)
-//   u16   slot[U][32]     its column's ring slot (slot R holds a constant 0)
-//   u16   oslot[32]       ring slot of the lane's row (lanes with sub-lane 0)
-//   int   xidx[32]        where x of the row goes (-1: nowhere, a warm-up row)
-//   T     inv[32]         1 / L_rr
-//   T     bv[32]          b of the row, written before each solve by
-//                         k_band_gather from bidx (the row whose b it is)
-// padded to 16 bytes.  The records of CH consecutive steps are one
-// contiguous chunk; lane 0 brings chunks into NST shared-memory stages with
-// cp.async.bulk (the bulk-copy engine, completion counted on an mbarrier),
-// NST - 1 chunks ahead of the warp.  The waits on the mbarriers are bounded
-// like every other wait of the library.
+// level at most U = 4 entries per lane); step t is one fixed-size record
+// holding, per lane, a packet of 16-byte pieces stored piece-major (see
+// band_rec_bytes): the lane's 4 entry values and their columns' slots (slot
+// R holds a constant 0 for unused entries), the slot and output row of the
+// lane's row (-1: a warm-up row, x goes nowhere), 1 / L_rr, the step's kp
+// and whether it ends its level, and b of the row, written before each solve
+// by k_band_gather from bidx (the row whose b it is).  A lane reads its
+// packet with 3-4 conflict-free 128-bit loads.  The records of CH
+// consecutive steps are one contiguous chunk; lane 0 brings chunks into NST
+// shared-memory stages with cp.async.bulk (the bulk-copy engine, completion
+// counted on an mbarrier), NST - 1 chunks ahead of the warp.  The waits on
+// the mbarriers are bounded like every other wait of the library.
 //
 // Slots.  A row's value lives in a shared-memory slot from its level until
 // the last level that reads it.  The builder hands slots out in the warp's
@@ -51,25 +49,19 @@ constexpr int kBandCH = 16;       // steps per chunk
 constexpr int kBandNST = 3;       // chunk stages in shared memory
 constexpr int kBandMaxRing = 8192;
 
-int rec_bytes(int U, int tsz)
+// Record of one step: per lane a packet of 16-byte pieces, stored piece-major
+// (piece k of lane j at k * 512 + j * 16), so a warp reads a piece with one
+// conflict-free 128-bit shared-memory load per lane.
+//   FP64 (4 pieces): {v0, v1} {v2, v3} {slot0|slot1, slot2|slot3, os|kp<<16|lend<<24, xi} {inv, bv}
+//   FP32 (3 pieces): {v0..v3} {slot0|slot1, slot2|slot3, os|kp<<16|lend<<24, xi} {inv, bv, 0, 0}
+// (slots and os 16 bits each; kp and lend are the step's, the same in every lane)
+__host__ __device__ constexpr int band_pieces(int tsz) { return tsz == 8 ? 4 : 3; }
+__host__ __device__ constexpr int band_rec_bytes(int tsz) { return band_pieces(tsz) * 512; }
+// byte offset of lane j's b inside a record
+__host__ __device__ constexpr size_t band_bv_offset(int tsz, int j)
 {
-    int b = 16 + U * 32 * tsz + U * 32 * 2 + 32 * 2 + 32 * 4 + 32 * tsz + 32 * tsz;
-    return (b + 15) & ~15;
+    return tsz == 8 ? 3 * 512 + (size_t)j * 16 + 8 : 2 * 512 + (size_t)j * 16 + 4;
 }
-
-struct RecView {
-    int U, tsz;
-    size_t off_val, off_slot, off_oslot, off_xidx, off_inv, off_bv;
-    RecView(int U_, int tsz_) : U(U_), tsz(tsz_)
-    {
-        off_val = 16;
-        off_slot = off_val + (size_t)U * 32 * tsz;
-        off_oslot = off_slot + (size_t)U * 32 * 2;
-        off_xidx = off_oslot + 64;
-        off_inv = off_xidx + 128;
-        off_bv = off_inv + (size_t)32 * tsz;
-    }
-};
 
 __device__ __forceinline__ unsigned smem_addr(const void* p)
 {
@@ -130,56 +122,80 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 
 // b of every step's rows into the records (T = the record value type).
 template <typename T, typename BT>
-__global__ void k_band_gather(unsigned char* rec, int rec_bytes, size_t off_bv, const int* __restrict__ bidx,
-                              long long nslots, const BT* __restrict__ b)
+__global__ void k_band_gather(unsigned char* rec, const int* __restrict__ bidx, long long nslots,
+                              const BT* __restrict__ b)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots;
          i += (long long)gridDim.x * blockDim.x) {
         const int r = bidx[i];
-        T* bv = reinterpret_cast<T*>(rec + (size_t)(i >> 5) * rec_bytes + off_bv);
-        bv[i & 31] = r >= 0 ? (T)b[r] : (T)0;
+        T* bv = reinterpret_cast<T*>(rec + (size_t)(i >> 5) * band_rec_bytes(sizeof(T)) +
+                                     band_bv_offset(sizeof(T), (int)(i & 31)));
+        *bv = r >= 0 ? (T)b[r] : (T)0;
     }
 }
 
-// One step's record fields of this lane, in registers.
-template <typename T, int U>
+// One step's record fields of this lane, in registers (U = 4).
+template <typename T>
 struct BandStep {
     int kp, lend, os, xi;
-    T v[U], bv, inv;
-    int sl[U];
-    __device__ __forceinline__ void load(const unsigned char* r, int lane, size_t off_val, size_t off_slot,
-                                         size_t off_oslot, size_t off_xidx, size_t off_inv, size_t off_bv)
+    T v[4], bv, inv;
+    int sl[4];
+    __device__ __forceinline__ void unpack_meta(const uint4& c)
     {
-        const int4 hdr = *reinterpret_cast<const int4*>(r);
-        kp = hdr.x;
-        lend = hdr.y;
-        const T* val = reinterpret_cast<const T*>(r + off_val);
-        const unsigned short* slot = reinterpret_cast<const unsigned short*>(r + off_slot);
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-            v[q] = val[q * 32 + lane];
-            sl[q] = slot[q * 32 + lane];
-        }
-        bv = reinterpret_cast<const T*>(r + off_bv)[lane];
-        os = reinterpret_cast<const unsigned short*>(r + off_oslot)[lane];
-        xi = reinterpret_cast<const int*>(r + off_xidx)[lane];
-        inv = reinterpret_cast<const T*>(r + off_inv)[lane];
+        sl[0] = (int)(c.x & 0xffffu);
+        sl[1] = (int)(c.x >> 16);
+        sl[2] = (int)(c.y & 0xffffu);
+        sl[3] = (int)(c.y >> 16);
+        os = (int)(c.z & 0xffffu);
+        kp = (int)((c.z >> 16) & 0xffu);
+        lend = (int)(c.z >> 24);
+        xi = (int)c.w;
     }
+    __device__ __forceinline__ void load(const unsigned char* r, int lane);
 };
+template <>
+__device__ __forceinline__ void BandStep<double>::load(const unsigned char* r, int lane)
+{
+    const uint4* p = reinterpret_cast<const uint4*>(r) + lane;
+    const uint4 c0 = p[0], c1 = p[32], c2 = p[64], c3 = p[96];
+    v[0] = __hiloint2double((int)c0.y, (int)c0.x);
+    v[1] = __hiloint2double((int)c0.w, (int)c0.z);
+    v[2] = __hiloint2double((int)c1.y, (int)c1.x);
+    v[3] = __hiloint2double((int)c1.w, (int)c1.z);
+    unpack_meta(c2);
+    inv = __hiloint2double((int)c3.y, (int)c3.x);
+    bv = __hiloint2double((int)c3.w, (int)c3.z);
+}
+template <>
+__device__ __forceinline__ void BandStep<float>::load(const unsigned char* r, int lane)
+{
+    const uint4* p = reinterpret_cast<const uint4*>(r) + lane;
+    const uint4 c0 = p[0], c1 = p[32], c2 = p[64];
+    v[0] = __uint_as_float(c0.x);
+    v[1] = __uint_as_float(c0.y);
+    v[2] = __uint_as_float(c0.z);
+    v[3] = __uint_as_float(c0.w);
+    unpack_meta(c1);
+    inv = __uint_as_float(c2.x);
+    bv = __uint_as_float(c2.y);
+}
 
 template <typename T, int U, int OUT>
-__global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restrict__ rec, int rec_bytes,
+__global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restrict__ rec,
                                                     const int* __restrict__ ustep, int nunits, int R, T* x,
                                                     double* x64, DevStatus* st, unsigned long long budget)
 {
+    constexpr int rec_bytes = band_rec_bytes(sizeof(T));
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ __align__(8) unsigned long long bars[kBandNST];
+    // a chunk's results, written to x at the chunk's end: a global store
+    // between two levels would make the level barrier wait for it
+    __shared__ T outv[kBandCH * 32];
+    __shared__ int outi[kBandCH * 32];
     const int lane = threadIdx.x;
     T* ring = reinterpret_cast<T*>(sm);
     unsigned char* stage = sm + (((size_t)(R + 1) * sizeof(T) + 15) & ~(size_t)15);
     const size_t chunk_bytes = (size_t)kBandCH * rec_bytes;
-    const size_t off_val = 16, off_slot = off_val + (size_t)U * 32 * sizeof(T), off_oslot = off_slot + U * 64,
-                 off_xidx = off_oslot + 64, off_inv = off_xidx + 128, off_bv = off_inv + 32 * sizeof(T);
     if (lane == 0) {
         for (int k = 0; k < kBandNST; k++) mbar_init(&bars[k], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -226,12 +242,10 @@ __global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restr
             // the record of step j + 1 is read into registers before step j
             // touches the slots, so its loads are not held behind step j's
             // shared-memory store (the compiler cannot tell the two apart)
-            BandStep<T, U> cur, nxt;
-            cur.load(cb, lane, off_val, off_slot, off_oslot, off_xidx, off_inv, off_bv);
+            BandStep<T> cur, nxt;
+            cur.load(cb, lane);
             for (int j = 0; j < steps; j++) {
-                if (j + 1 < steps)
-                    nxt.load(cb + (size_t)(j + 1) * rec_bytes, lane, off_val, off_slot, off_oslot, off_xidx, off_inv,
-                             off_bv);
+                if (j + 1 < steps) nxt.load(cb + (size_t)(j + 1) * rec_bytes, lane);
                 // two partial sums halve the dependent multiply-add chain
                 T a0 = cur.bv, a1 = (T)0;
 #pragma unroll
@@ -241,17 +255,29 @@ __global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restr
                 }
                 T acc = a0 + a1;
                 for (int o = cur.kp >> 1; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                int oi = -1;
                 if ((lane & (cur.kp - 1)) == 0 && cur.os < R) {
                     const T xv = acc * cur.inv;
                     ring[cur.os] = xv;
-                    if (cur.xi >= 0) {
-                        if (x) x[cur.xi] = xv;
-                        if (OUT == OUT_SET64) x64[cur.xi] = (double)xv;
-                        if (OUT == OUT_ADD64) x64[cur.xi] += (double)xv;
-                    }
+                    outv[j * 32 + lane] = xv;
+                    oi = cur.xi;
                 }
+                outi[j * 32 + lane] = oi;
                 if (cur.lend) __syncwarp();
                 cur = nxt;
+            }
+            // the chunk's results to x (each lane its own slots of the buffer)
+#pragma unroll
+            for (int j = 0; j < kBandCH; j++) {
+                if (j < steps) {
+                    const int i = outi[j * 32 + lane];
+                    if (i >= 0) {
+                        const T v = outv[j * 32 + lane];
+                        if (x) x[i] = v;
+                        if (OUT == OUT_SET64) x64[i] = (double)v;
+                        if (OUT == OUT_ADD64) x64[i] += (double)v;
+                    }
+                }
             }
             __syncwarp();
         }
@@ -282,7 +308,7 @@ int band_launch_t(const BandLayout& t, const unsigned char* rec, int rb, T* x, d
     auto kern = k_sptrsv_band<T, kBandU, OUT>;
     const size_t smem = (((size_t)(t.R + 1) * sizeof(T) + 15) & ~(size_t)15) + (size_t)kBandNST * kBandCH * rb;
     SPT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<t.nunits, 32, smem, s>>>(rec, rb, t.ustep, t.nunits, t.R, x, x64, c->d_status, wait_budget_ns());
+    kern<<<t.nunits, 32, smem, s>>>(rec, t.ustep, t.nunits, t.R, x, x64, c->d_status, wait_budget_ns());
     SPT_CUDA(cudaGetLastError());
     return 0;
 }
@@ -428,31 +454,22 @@ int build_band_layout(sptrsv_plan_s* p)
     for (int un = 0; un < nunits; un++)
         for (int r = u0[un]; r < u0[un + 1]; r++) unit_of[r] = un;
     const long long ns = (long long)steps.size();
-    const int rb64 = rec_bytes(U, 8), rb32 = rec_bytes(U, 4);
+    const int rb64 = band_rec_bytes(8), rb32 = band_rec_bytes(4);
     std::vector<unsigned char> h64((size_t)ns * rb64, 0), h32((size_t)ns * rb32, 0);
     std::vector<int> bidx((size_t)ns * 32, -1);
-    const RecView V64(U, 8), V32(U, 4);
     for (long long t = 0; t < ns; t++) {
         const Step& sp = steps[t];
         unsigned char* r64 = &h64[(size_t)t * rb64];
         unsigned char* r32 = &h32[(size_t)t * rb32];
-        const int hdr[4] = {sp.kp, sp.level_end, sp.cnt, 0};
-        memcpy(r64, hdr, 16);
-        memcpy(r32, hdr, 16);
-        auto* v64 = reinterpret_cast<double*>(r64 + V64.off_val);
-        auto* v32 = reinterpret_cast<float*>(r32 + V32.off_val);
-        auto* s64 = reinterpret_cast<unsigned short*>(r64 + V64.off_slot);
-        auto* s32 = reinterpret_cast<unsigned short*>(r32 + V32.off_slot);
-        auto* o64 = reinterpret_cast<unsigned short*>(r64 + V64.off_oslot);
-        auto* o32 = reinterpret_cast<unsigned short*>(r32 + V32.off_oslot);
-        auto* x64 = reinterpret_cast<int*>(r64 + V64.off_xidx);
-        auto* x32 = reinterpret_cast<int*>(r32 + V32.off_xidx);
-        auto* i64 = reinterpret_cast<double*>(r64 + V64.off_inv);
-        auto* i32 = reinterpret_cast<float*>(r32 + V32.off_inv);
+        // per lane: values, slots (R: the constant-0 slot), row slot, output row, 1/L_rr
+        double v[32][4] = {};
+        int sl[32][4], os[32], xi[32];
+        double inv[32] = {};
+        float invf[32] = {};
         for (int j = 0; j < 32; j++) {
-            o64[j] = o32[j] = (unsigned short)R;  // no row: slot R is never written
-            x64[j] = x32[j] = -1;
-            for (int q = 0; q < U; q++) s64[q * 32 + j] = s32[q * 32 + j] = (unsigned short)R;
+            for (int q = 0; q < 4; q++) sl[j][q] = R;
+            os[j] = R;  // no row: slot R is never written
+            xi[j] = -1;
         }
         for (int w = 0; w < sp.cnt; w++) {
             const int r = all_order[sp.first + w];
@@ -462,18 +479,32 @@ int build_band_layout(sptrsv_plan_s* p)
             for (int q = rp[r]; q < d; q++) {
                 const int k = q - rp[r];
                 const int lane = lane0 + (k % sp.kp), uu = k / sp.kp;
-                const int sl = slot_of[ci[q]];
-                s64[uu * 32 + lane] = s32[uu * 32 + lane] = (unsigned short)sl;
-                v64[uu * 32 + lane] = va[q];
-                v32[uu * 32 + lane] = (float)va[q];
+                sl[lane][uu] = slot_of[ci[q]];
+                v[lane][uu] = va[q];
             }
             bool real = true;
             const int orow = outer_row(un, r, &real);
-            o64[lane0] = o32[lane0] = (unsigned short)slot_of[r];
-            x64[lane0] = x32[lane0] = real ? orow : -1;
-            i64[lane0] = 1.0 / va[d];
-            i32[lane0] = 1.0f / (float)va[d];
+            os[lane0] = slot_of[r];
+            xi[lane0] = real ? orow : -1;
+            inv[lane0] = 1.0 / va[d];
+            invf[lane0] = 1.0f / (float)va[d];
             bidx[(size_t)t * 32 + lane0] = orow;
+        }
+        for (int j = 0; j < 32; j++) {
+            const unsigned meta[4] = {(unsigned)sl[j][0] | ((unsigned)sl[j][1] << 16),
+                                      (unsigned)sl[j][2] | ((unsigned)sl[j][3] << 16),
+                                      (unsigned)os[j] | ((unsigned)sp.kp << 16) | ((unsigned)sp.level_end << 24),
+                                      (unsigned)xi[j]};
+            // FP64 pieces
+            memcpy(r64 + 0 * 512 + j * 16, &v[j][0], 16);
+            memcpy(r64 + 1 * 512 + j * 16, &v[j][2], 16);
+            memcpy(r64 + 2 * 512 + j * 16, meta, 16);
+            memcpy(r64 + 3 * 512 + j * 16, &inv[j], 8);
+            // FP32 pieces
+            const float vf[4] = {(float)v[j][0], (float)v[j][1], (float)v[j][2], (float)v[j][3]};
+            memcpy(r32 + 0 * 512 + j * 16, vf, 16);
+            memcpy(r32 + 1 * 512 + j * 16, meta, 16);
+            memcpy(r32 + 2 * 512 + j * 16, &invf[j], 4);
         }
     }
     BandLayout t;
@@ -512,19 +543,14 @@ int band_solve(sptrsv_plan_s* p, bool f32, const void* b, bool b_f32, void* x, d
     const long long nslots = (long long)t.nsteps * 32;
     const int g = grid_for(nslots, 256);
     if (!f32) {
-        const RecView V(kBandU, 8);
-        k_band_gather<double, double><<<g, 256, 0, s>>>(t.rec64, t.rb64, V.off_bv, t.bidx, nslots,
-                                                        static_cast<const double*>(b));
+        k_band_gather<double, double><<<g, 256, 0, s>>>(t.rec64, t.bidx, nslots, static_cast<const double*>(b));
         SPT_CUDA(cudaGetLastError());
         return band_launch_t<double, OUT_X>(t, t.rec64, t.rb64, static_cast<double*>(x), nullptr, s);
     }
-    const RecView V(kBandU, 4);
     if (b_f32)
-        k_band_gather<float, float><<<g, 256, 0, s>>>(t.rec32, t.rb32, V.off_bv, t.bidx, nslots,
-                                                      static_cast<const float*>(b));
+        k_band_gather<float, float><<<g, 256, 0, s>>>(t.rec32, t.bidx, nslots, static_cast<const float*>(b));
     else
-        k_band_gather<float, double><<<g, 256, 0, s>>>(t.rec32, t.rb32, V.off_bv, t.bidx, nslots,
-                                                       static_cast<const double*>(b));
+        k_band_gather<float, double><<<g, 256, 0, s>>>(t.rec32, t.bidx, nslots, static_cast<const double*>(b));
     SPT_CUDA(cudaGetLastError());
     float* xf = static_cast<float*>(x);
     if (out_mode == OUT_SET64) return band_launch_t<float, OUT_SET64>(t, t.rec32, t.rb32, xf, x64, s);

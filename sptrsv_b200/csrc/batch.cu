@@ -1427,7 +1427,7 @@ int sptrsv_batch_solve_graph(sptrsv_batch_t B, const double* b, double* x, int p
 
 namespace sptrsv {
 int partition_blocks(const int* rp, const int* ci, const double* va, int n, int P, int threads, std::vector<int>& tab,
-                     int* reach, double* bound);
+                     int* reach, double* bound, double min_ratio);
 }
 
 extern "C" {
@@ -1488,7 +1488,8 @@ int sptrsv_batch_set_partition(sptrsv_batch_t B, int block_rows)
                     std::vector<int> tab;
                     int w = 0;
                     double bnd = 0;
-                    if (partition_blocks(rp.data(), ci.data(), va.data(), ns, P, 1, tab, &w, &bnd) == 0) {
+                    // blocks at least twice their warm-up, else the warm-ups would dominate
+                    if (partition_blocks(rp.data(), ci.data(), va.data(), ns, P, 1, tab, &w, &bnd, 2.0) == 0) {
                         tabs[sy] = tab;
                         bounds[sy] = bnd;
                     }

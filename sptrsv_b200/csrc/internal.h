@@ -90,7 +90,9 @@ cudaError_t launch_persistent_capped(void (*kern)(KArgs...), int block, size_t s
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) cudaGetLastError();  // reported here; not left for the next check to find
+    return e;
 }
 
 template <typename... KArgs, typename... Args>

@@ -25,7 +25,7 @@
 //             in FP64 with rounding error below the second term (m: most
 //             off-diagonals of a row, u = 2^-53); far tighter when signs
 //             cancel (random values), and used when its dense rows are cheap
-//             (at most 512 coupled columns).
+//             (coupled columns x most off-diagonals of a row <= 4096).
 // Window argument: let w be the reach of L (most rows between an entry's
 // column and its row).  A row r >= a + w depends only on rows in
 // [r - w, r), all past s; with |L_rr| >= sum_j |L_rj| its bound is at most
@@ -52,7 +52,7 @@ namespace sptrsv {
 namespace {
 
 constexpr double kPartEps = 0x1p-60;
-constexpr int kSpikeMaxCols = 512;
+constexpr long long kSpikeMaxWork = 4096;  // coupled columns x most off-diagonals of a row
 
 struct HostCsr {
     int n = 0;
@@ -156,10 +156,12 @@ int run_start_below(const std::vector<unsigned char>& run0, int r, int span)
     return r;
 }
 
-// Smallest warm-up start s for block [a, e) (searched from the guess K0):
-// doubling, then bisection.  Returns s (0 = exact) and the bound in *bnd.
+// Smallest warm-up start s for block [a, e) (searched from the guess K0).
+// refine: doubling, then bisection (a search from scratch); otherwise the
+// guess (a neighbouring block's warm-up) is tried at 9/10 and grown by 6/5
+// until the bound holds.  Returns s (0 = exact) and the bound in *bnd.
 int find_start(const HostCsr& L, const std::vector<unsigned char>& run0, int a, int e, int w, int maxoff,
-               bool spike, int K0, double* bnd)
+               bool spike, int K0, double* bnd, bool refine = true)
 {
     auto start_for = [&](long long K) {
         long long s = (long long)a - K;
@@ -167,6 +169,24 @@ int find_start(const HostCsr& L, const std::vector<unsigned char>& run0, int a, 
         return run_start_below(run0, (int)s, w);
     };
     long long K = std::max<long long>(K0, w);
+    if (!refine) {
+        const long long Kd = std::max<long long>(w, K * 9 / 10);
+        int sd = start_for(Kd);
+        double bd = sd == 0 ? 0.0 : block_bound(L, sd, a, e, w, maxoff, spike);
+        if (bd <= kPartEps) {
+            *bnd = bd;
+            return sd;
+        }
+        for (;;) {
+            const int sk = start_for(K);
+            const double bk = sk == 0 ? 0.0 : block_bound(L, sk, a, e, w, maxoff, spike);
+            if (bk <= kPartEps) {
+                *bnd = bk;
+                return sk;
+            }
+            K = std::max<long long>(K * 6 / 5, K + w);
+        }
+    }
     int s = start_for(K);
     double b = block_bound(L, s, a, e, w, maxoff, spike);
     long long lo = 0, hi;
@@ -265,24 +285,32 @@ int download_natural_csr(sptrsv_plan_s* p, std::vector<int>& rp, std::vector<int
     return 0;
 }
 
-void part_free(sptrsv_plan_s* p)
+static void part_delete(PartPlan* q)
 {
-    PartPlan* q = p->part;
     if (!q) return;
     if (q->sub) sptrsv_plan_destroy(q->sub);
     if (q->info.row_ctr || q->ext.ia) free_device_analysis(&q->ext, &q->info);
     cudaFree(q->d_tab);
     cudaFree(q->bx); cudaFree(q->xx); cudaFree(q->bx32); cudaFree(q->xx32);
     delete q;
-    p->part = nullptr;
+}
+
+void part_free(sptrsv_plan_s* p)
+{
+    part_delete(p->part);
+    part_delete(p->part_alt);
+    p->part = p->part_alt = nullptr;
 }
 
 // Blocks of a host CSR (natural order, diagonal last): P block starts near
 // i n / P at run starts, and each block's warm-up start.  tab gets 4 ints per
 // block (s, a, e, 0); *reach, *bound as in PartPlan.  threads: host threads
-// for the per-block searches (1: the caller's thread only).
+// for the per-block searches (1: the caller's thread only).  min_ratio > 0:
+// the warm-up is first measured on a probe block in the middle of the
+// matrix, and P is lowered so that blocks hold at least min_ratio times it
+// (SPTRSV_ERR_UNSUPPORTED when fewer than 2 blocks remain).
 int partition_blocks(const int* rp, const int* ci, const double* va, int n, int P, int threads,
-                     std::vector<int>& tab, int* reach, double* bound)
+                     std::vector<int>& tab, int* reach, double* bound, double min_ratio)
 {
     if (P < 2 || P > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "partitions: P must be in [2, 4096]");
     if ((long long)n < 64LL * P)
@@ -308,6 +336,20 @@ int partition_blocks(const int* rp, const int* ci, const double* va, int n, int 
             return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: row %d is not diagonally dominant "
                              "(|L_ii| < sum |L_ij|); a partitioned solve needs every row to be", r);
     }
+    // the bound costs a dense row of the spike per row: used when that is cheap
+    const bool spike = (long long)std::min(w, n) * std::max(1, maxoff) <= kSpikeMaxWork;
+    int Kprobe = 0;
+    if (min_ratio > 0) {
+        const int ap = run_start_below(run0, n / 2, w);
+        double bp = 0;
+        const int sp = find_start(L, run0, ap, std::min(n, ap + n / P), w, maxoff, spike, 2 * w, &bp);
+        Kprobe = ap - sp;
+        const long long Pmax = (long long)(n / (min_ratio * std::max(1, Kprobe)));
+        if (Pmax < P) P = (int)Pmax;
+        if (P < 2)
+            return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: a warm-up of %d rows leaves no room for 2 blocks",
+                             Kprobe);
+    }
     // block starts: run starts near i n / P
     std::vector<int> a(P + 1);
     a[0] = 0;
@@ -329,17 +371,18 @@ int partition_blocks(const int* rp, const int* ci, const double* va, int n, int 
     }
     for (int i = 1; i <= P; i++)
         if (a[i] <= a[i - 1]) return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: empty block");
-    // warm-up starts: block 1 searched from scratch, the rest from its result, in parallel
-    const bool spike = std::min(w, n) <= kSpikeMaxCols;
+    // warm-up starts: block 1 searched from scratch (or from the probe), the
+    // rest from its result, in parallel
     std::vector<int> s(P, 0);
     std::vector<double> bnd(P, 0.0);
-    s[1] = find_start(L, run0, a[1], a[2], w, maxoff, spike, 2 * w, &bnd[1]);
-    const int K1 = a[1] - s[1];
+    s[1] = find_start(L, run0, a[1], a[2], w, maxoff, spike, Kprobe > 0 ? Kprobe : 2 * w, &bnd[1], Kprobe == 0);
+    const int K1 = std::max(a[1] - s[1], Kprobe);
     {
         const int nt = std::max(1, std::min<int>(P - 2, threads));
         std::vector<std::thread> th;
         auto work = [&](int t) {
-            for (int i = 2 + t; i < P; i += nt) s[i] = find_start(L, run0, a[i], a[i + 1], w, maxoff, spike, K1, &bnd[i]);
+            for (int i = 2 + t; i < P; i += nt)
+                s[i] = find_start(L, run0, a[i], a[i + 1], w, maxoff, spike, K1, &bnd[i], false);
         };
         if (nt == 1) {
             work(0);
@@ -364,11 +407,18 @@ int partition_blocks(const int* rp, const int* ci, const double* va, int n, int 
 int build_part(sptrsv_plan_s* p, int P)
 {
     if (p->part && p->part->P == P) return 0;
-    part_free(p);
+    // the two most recent block systems are kept (an autotuner alternates them)
+    if (p->part_alt && p->part_alt->P == P) {
+        std::swap(p->part, p->part_alt);
+        return 0;
+    }
+    part_delete(p->part_alt);
+    p->part_alt = p->part;
+    p->part = nullptr;
     const int n = p->n;
     if (P < 2 || P > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "partitions: P must be in [2, 4096]");
-    if ((long long)n < 64LL * P)
-        return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: %d rows are too few for %d blocks", n, P);
+    if ((long long)n < 256LL * P)  // blocks of fewer rows would be mostly warm-up
+        return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: %d rows are too few for %d blocks of >= 256 rows", n, P);
     HostCsr L;
     int e = download_natural(p, L);
     if (e) return e;
@@ -376,7 +426,7 @@ int build_part(sptrsv_plan_s* p, int P)
     int w = 0;
     double bound = 0;
     e = partition_blocks(L.rp.data(), L.ci.data(), L.va.data(), n, P, (int)std::thread::hardware_concurrency(), tab,
-                         &w, &bound);
+                         &w, &bound, 0.0);
     if (e) return e;
     std::vector<int> s(P), a(P + 1);
     for (int i = 0; i < P; i++) {
@@ -425,7 +475,8 @@ int build_part(sptrsv_plan_s* p, int P)
     }
     p->part = q;
     auto fail = [&](int code) {
-        part_free(p);
+        part_delete(p->part);
+        p->part = nullptr;
         return code;
     };
     e = allocate_memory(erp.data(), eci.data(), eva.data(), q->n_ext, &q->ext, ALL);

@@ -70,6 +70,9 @@ struct WaveLayout {
     int* grun = nullptr;       // [ngroups+1] first run of each group
     int* grow = nullptr;       // [ngroups+1] first row of each group
     int* gseq = nullptr;       // [ngroups] processing order of the groups (null: natural order)
+    int* brow = nullptr;       // block systems only: [nch*32] outer row whose b a slot takes
+    int* ghx = nullptr;        // block systems only: [ngroups*2] outer row of a group's first row,
+                               // its first row that is not a warm-up row
     int ngroups = 0, G = 0, cap = 0;  // cap: most rows in one group
     int maxe = 0;                      // most entries of one slot
 };
@@ -166,6 +169,7 @@ struct sptrsv_plan_s {
     int cap_host = 0;
     sptrsv_schedule_t sched{};
     PartPlan* part = nullptr;    // partitioned solve (sched.partitions >= 2)
+    PartPlan* part_alt = nullptr;  // the previous block system, kept for a switch back
     // set on a block system's plan: the first row of every block (WAVE
     // groups never span two blocks, and the blocks' groups are interleaved)
     std::vector<int> blk_starts;
@@ -208,6 +212,8 @@ int band_solve(sptrsv_plan_s* p, bool f32, const void* b, bool b_f32, void* x, d
 // not row diagonally dominant or too small to cut.
 int build_part(sptrsv_plan_s* p, int P);
 void part_free(sptrsv_plan_s* p);
+// Block-system vectors for nrhs right-hand sides (kept, grown on demand).
+int part_ensure(PartPlan* q, int k);
 // Partitioned solves (p->sched.partitions >= 2, p->part built).
 int part_solve_f64(sptrsv_plan_s* p, const double* b, double* x, int nrhs, cudaStream_t s);
 // FP32 solve of the block system for rhs (FP64 or FP32, n x nrhs): out32 =

@@ -226,12 +226,23 @@ int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cuda
     // so the time the host spends queueing the copies overlaps the solve
     SPT_CUDA(cudaEventRecord(p->ev_start, s));
     SPT_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_start, 0));
-    p->launch_bflag = p->bflag;
-    p->launch_epoch = p->epoch;
-    p->launch_hx = hx_dev;
-    int e = plan_solve_f64(p, p->hb, p->hx, 1, s);
-    p->launch_bflag = nullptr;
-    p->launch_hx = nullptr;
+    // a partitioned plan streams through its block system: that plan's WAVE
+    // layout maps each slot to the outer row of its b and each group to the
+    // outer rows of its real rows
+    sptrsv_plan_s* lp = p;
+    double* xbuf = p->hx;
+    if (p->part && p->sched.partitions >= 2) {
+        lp = p->part->sub;
+        int e = part_ensure(p->part, 1);
+        if (e) return e;
+        xbuf = p->part->xx;
+    }
+    lp->launch_bflag = p->bflag;
+    lp->launch_epoch = p->epoch;
+    lp->launch_hx = hx_dev;
+    int e = plan_solve_f64(lp, p->hb, xbuf, 1, s);
+    lp->launch_bflag = nullptr;
+    lp->launch_hx = nullptr;
     if (e) return e;
     for (int g = 0; g < nseg; g++) {
         const size_t r0 = (size_t)g * kStreamSegRows, rows = std::min<size_t>(kStreamSegRows, n - r0);
@@ -395,7 +406,10 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
                       f32 ? reinterpret_cast<const V*>(t.ev32) : reinterpret_cast<const V*>(t.ev64),
                       f32 ? reinterpret_cast<const V*>(t.lsub32) : reinterpret_cast<const V*>(t.lsub64),
                       f32 ? reinterpret_cast<const V*>(t.di32) : reinterpret_cast<const V*>(t.di64), nullptr},
-                     t.runc, t.grun, t.grow, t.gseq};
+                     t.runc, t.grun, t.grow,
+                     // a streamed solve takes the groups in row order, the order b arrives in
+                     p->launch_bflag ? nullptr : t.gseq, p->launch_bflag ? t.brow : nullptr,
+                     p->launch_bflag ? t.ghx : nullptr};
         auto kern = p->launch_bflag
                         ? (t.maxe <= 2         ? k_sptrsv_wave<V, T, BT, OUT, 2, false, true>
                            : t.maxe <= kStripU ? k_sptrsv_wave<V, T, BT, OUT, kStripU, false, true>
@@ -436,9 +450,12 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         const bool cg = (nrhs * sizeof(T)) % 16 == 0;
         auto kern = U == 8 ? (cg ? k_sptrsv_mrhs<V, T, BT, OUT, 8, MRHS_CG> : k_sptrsv_mrhs<V, T, BT, OUT, 8, MRHS_CA>)
                            : (cg ? k_sptrsv_mrhs<V, T, BT, OUT, 16, MRHS_CG> : k_sptrsv_mrhs<V, T, BT, OUT, 16, MRHS_CA>);
-        const size_t smem = (size_t)wpb * U * 32 * sizeof(T);
+        // the multi-RHS kernel takes at most 8 warps per block (its register use)
+        const int mw = std::min(wpb, 8), mblock = 32 * mw;
+        const int mcap = sc.warps_per_sm > 0 ? (sc.warps_per_sm + mw - 1) / mw : 0;
+        const size_t smem = (size_t)mw * U * 32 * sizeof(T);
         SPT_CUDA(allow_smem(kern, smem));
-        SPT_CUDA(launch_persistent_capped(kern, block, smem, div_up(t.ntasks, wpb), cap, s, ml, t.ntasks,
+        SPT_CUDA(launch_persistent_capped(kern, mblock, smem, div_up(t.ntasks, mw), mcap, s, ml, t.ntasks,
                                           reinterpret_cast<const MrhsTask*>(t.tasks), nrhs, kp, b, x, x64,
                                           reinterpret_cast<T*>(t.pbuf), t.pcnt, c->d_status, budget, backoff));
         return 0;
@@ -492,7 +509,6 @@ int plan_residual(sptrsv_plan_s* p, const double* b, const double* x, float* r32
 
 static bool partitioned(const sptrsv_plan_s* p) { return p->part && p->sched.partitions >= 2; }
 
-int part_ensure(PartPlan* q, int k);
 int part_gather64(PartPlan* q, const double* src, double* dst, int k, cudaStream_t s);
 int part_gather32(PartPlan* q, const float* src, float* dst, int k, cudaStream_t s);
 int part_scatter64(PartPlan* q, const double* src, double* dst, int k, cudaStream_t s);
@@ -887,9 +903,9 @@ int sptrsv_solve_host(sptrsv_plan_t p, const double* hb, double* hx, int nrhs, i
         p->cap_host = nrhs;
     }
     void* hx_dev = nullptr;
-    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && !partitioned(p) && mapped_host(hb) &&
+    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && mapped_host(hb) &&
         (hx_dev = mapped_host(hx)) != nullptr) {
-        int e = build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
+        int e = partitioned(p) ? 0 : build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
         if (!e) e = solve_host_streamed(p, hb, (double*)hx_dev, s);
         if (e) return e;
         e = sync_status(s);

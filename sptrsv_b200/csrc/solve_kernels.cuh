@@ -586,6 +586,7 @@ constexpr int kStripU = 4;
 template <typename T>
 struct StripMeta {
     int row, e0, e1;
+    int brow;  // row of b (row itself, except in a block system's streamed solve)
     T piv, lsub;
 };
 
@@ -600,6 +601,7 @@ template <typename V, typename T>
 __device__ __forceinline__ void strip_meta(StripMeta<T>& z, const StripMat<V>& m, int slot)
 {
     z.row = __ldg(m.row + slot);
+    z.brow = z.row;
     z.e0 = __ldg(m.pe + slot);
     z.e1 = __ldg(m.pe + slot + 1);
     z.piv = (T)__ldg(m.di + slot);
@@ -610,7 +612,7 @@ template <typename V, typename T, typename BT, int U = kStripU>
 __device__ __forceinline__ void strip_ent(StripEnt<T, U>& z, const StripMeta<T>& md, const StripMat<V>& m,
                                           const BT* __restrict__ b, bool coherent_b = false)
 {
-    z.b = md.row >= 0 ? (T)(coherent_b ? ld_relaxed(b + md.row) : b[md.row]) : (T)0;
+    z.b = md.row >= 0 ? (T)(coherent_b ? ld_relaxed(b + md.brow) : b[md.brow]) : (T)0;
 #pragma unroll
     for (int u = 0; u < U; u++) {
         z.cc[u] = 0;
@@ -726,6 +728,11 @@ struct WaveMat {
     const int* __restrict__ grun;  // first run of each group
     const int* __restrict__ grow;  // first row of each group
     const int* __restrict__ gseq;  // processing order of the groups (null: natural)
+    // streamed solves of a block system (else null): per slot the outer row
+    // whose b it takes, per group {outer row of its first row, its first row
+    // that is not a warm-up row}
+    const int* __restrict__ brow;
+    const int* __restrict__ ghx;
 };
 
 template <typename V, typename T, typename BT, int OUT, int U, bool MULTI, bool STREAM>
@@ -763,7 +770,8 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
             StripMeta<T> m0, m1;
             StripEnt<T, U> e0;
             strip_meta<V, T>(m0, m, q0 * 32 + lane);
-            if (!b_ready(m0.row)) failed = true;
+            if (STREAM && w.brow && m0.row >= 0) m0.brow = __ldg(w.brow + q0 * 32 + lane);
+            if (!b_ready(m0.row >= 0 ? m0.brow : -1)) failed = true;
             strip_ent<V, T, BT, U>(e0, m0, m, b, STREAM);
             if (q0 + 1 < q1) strip_meta<V, T>(m1, m, (q0 + 1) * 32 + lane);
             for (int q = q0; q < q1 && !failed; q++) {
@@ -771,7 +779,8 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
                 const StripEnt<T, U> en = e0;
                 if (q + 1 < q1) {
                     m0 = m1;
-                    if (!b_ready(m0.row)) {
+                    if (STREAM && w.brow && m0.row >= 0) m0.brow = __ldg(w.brow + (q + 1) * 32 + lane);
+                    if (!b_ready(m0.row >= 0 ? m0.brow : -1)) {
                         failed = true;
                         break;
                     }
@@ -827,8 +836,10 @@ __global__ void __launch_bounds__(512, 1) k_sptrsv_wave(WaveMat<V> w, int ngroup
         __syncthreads();
         if (abort_flag) return;
         // each thread copies the slots it refills with the sentinel for the next group
-        if (STREAM && hx)
-            for (int t = threadIdx.x; t < nr; t += blockDim.x) hx[r0 + t] = (double)xs[t];
+        if (STREAM && hx) {
+            const int o = w.ghx ? __ldg(w.ghx + 2 * g) : r0, t0 = w.ghx ? __ldg(w.ghx + 2 * g + 1) : 0;
+            for (int t = t0 + threadIdx.x; t < nr; t += blockDim.x) hx[o + t] = (double)xs[t];
+        }
     }
 }
 

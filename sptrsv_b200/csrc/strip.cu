@@ -187,7 +187,7 @@ void wave_free(WaveLayout& w)
 {
     cudaFree(w.row); cudaFree(w.pe); cudaFree(w.ecol); cudaFree(w.ev64); cudaFree(w.ev32); cudaFree(w.lsub64);
     cudaFree(w.lsub32); cudaFree(w.di64); cudaFree(w.di32); cudaFree(w.runc); cudaFree(w.grun); cudaFree(w.grow);
-    cudaFree(w.gseq);
+    cudaFree(w.gseq); cudaFree(w.brow); cudaFree(w.ghx);
     w = WaveLayout{};
 }
 
@@ -531,6 +531,38 @@ int build_wave_layout(sptrsv_plan_s* p, int G, int max_rows)
                                                       w.ev64, w.ev32);
     WCHK(cudaGetLastError());
     WCHK(cudaStreamSynchronize(s));
+    if (!p->part_tab.empty() && ngroups > 0) {
+        // a block system: b rows and x destinations in the outer plan's rows,
+        // for its streamed host solves
+        const int P = (int)p->part_tab.size() / 4;
+        auto blk = [&](int row) {  // block holding a block-system row
+            int lo = 0, hi = P - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (p->part_tab[4 * mid + 3] <= row) lo = mid;
+                else hi = mid - 1;
+            }
+            return lo;
+        };
+        std::vector<int> hrow(nslots), hbrow(nslots, -1), hghx(2 * (size_t)ngroups);
+        WCHK(cudaMemcpy(hrow.data(), w.row, sizeof(int) * (size_t)nslots, cudaMemcpyDeviceToHost));
+        for (int q = 0; q < nslots; q++)
+            if (hrow[q] >= 0) {
+                const int b = blk(hrow[q]);
+                hbrow[q] = p->part_tab[4 * b] + (hrow[q] - p->part_tab[4 * b + 3]);
+            }
+        for (int g = 0; g < ngroups; g++) {
+            const int b = blk(grow[g]);
+            const int sb = p->part_tab[4 * b], ab = p->part_tab[4 * b + 1], base = p->part_tab[4 * b + 3];
+            const int nr = grow[g + 1] - grow[g];
+            hghx[2 * g] = sb + (grow[g] - base);
+            hghx[2 * g + 1] = std::max(0, std::min(nr, base + (ab - sb) - grow[g]));
+        }
+        WCHK(dalloc(&w.brow, nslots));
+        WCHK(dalloc(&w.ghx, 2LL * ngroups));
+        WCHK(cudaMemcpy(w.brow, hbrow.data(), sizeof(int) * (size_t)nslots, cudaMemcpyHostToDevice));
+        WCHK(cudaMemcpy(w.ghx, hghx.data(), sizeof(int) * 2 * (size_t)ngroups, cudaMemcpyHostToDevice));
+    }
 #undef WCHK
     w.ngroups = ngroups;
     w.G = G;

@@ -1,15 +1,17 @@
 // tune.cu — the schedule classes, the exhaustive autotuner and the MLP's
 // schedule prediction.
 //
-// 24 classes = 4 groups x 6 parameter presets.  The natural-order group holds
-// SIMPLE with 1 and 32 rows per task, STRIP with one grid line per warp and
-// WAVE with 4, 8 and 16 grid lines per CTA (STRIP and WAVE apply only to
-// matrices with their chunk structure, WAVE only where a line group fits
-// shared memory; elsewhere those classes fail to set and are skipped).  For
-// ORDER the preset is rows per warp (1..32, i.e. 32..1 lanes per row — the
-// reference's six tile sizes, analysis_csr.cu:84-102).  MULTIROW takes lanes per row from the analysis
-// map, so its presets vary the polling back-off and the number of resident
-// warps.  CLUSTER presets vary band height, cluster size and lanes per row.
+// 24 classes = 4 groups x 6 parameter presets (one table, below).  The
+// natural-order group holds SIMPLE, STRIP and WAVE, whole and over 16 blocks
+// with warm-ups (STRIP and WAVE apply only to matrices with their chunk
+// structure, WAVE only where a line group fits shared memory; elsewhere those
+// classes fail to set and are skipped).  For ORDER the preset is rows per
+// warp (1..32, i.e. 32..1 lanes per row — the reference's six tile sizes,
+// analysis_csr.cu:84-102).  MULTIROW takes lanes per row from the analysis
+// map; its presets vary the polling back-off and resident warps, and cut the
+// rows into 16 or 128 blocks.  The last group holds CLUSTER and BAND, whole
+// and over blocks.  Partitioned classes use 16 or 128 blocks only, so an
+// autotune builds at most two block systems (a plan keeps the last two).
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -30,45 +32,38 @@ extern "C" {
 int sptrsv_schedule_from_class(int cls, sptrsv_schedule_t* s)
 {
     if (!s || cls < 0 || cls >= SPTRSV_N_CLASSES) return set_error(SPTRSV_ERR_INVALID_ARG, "schedule_from_class: bad class");
-    static const int rpw[6] = {1, 2, 4, 8, 16, 32};
-    // natural-order group: SIMPLE with 1 and 32 rows per task; between them
-    // STRIP with one grid line per warp and WAVE with 4, 8, 16 lines per CTA
-    static const int nat_v[6] = {SPTRSV_VAR_SIMPLE, SPTRSV_VAR_STRIP, SPTRSV_VAR_WAVE, SPTRSV_VAR_WAVE,
-                                 SPTRSV_VAR_WAVE, SPTRSV_VAR_SIMPLE};
-    static const int nat_bw[6] = {8, 2, 4, 8, 16, 8};
-    // MULTIROW presets: block warps, back-off ns, resident warps per SM
-    static const int mr[6][3] = {{8, 0, 0}, {8, 200, 0}, {8, 1000, 0}, {4, 0, 16}, {8, 200, 32}, {16, 0, 0}};
-    // CLUSTER presets: band levels, cluster rows, rows per warp, block warps
-    // (from sweeps of H = 16..4096, B = 1024..8192 on banded and grid matrices:
-    // wide bands with 16 rows per task and 16-warp blocks lead)
-    static const int cl[6][4] = {{64, 4096, 16, 8},    {128, 4096, 16, 16}, {256, 2048, 16, 16},
-                                 {256, 4096, 16, 16},  {512, 8192, 16, 16}, {4096, 2048, 16, 8}};
-    const int v = cls / 6, j = cls % 6;
-    s->variant = v;
-    s->rows_per_warp = 1;
-    s->block_warps = 8;
-    s->warps_per_sm = 0;
-    s->backoff_ns = 0;
+    // preset: {variant, rows_per_warp, block_warps, warps_per_sm, backoff_ns, band_levels, cluster_rows, partitions}
+    static const int T[SPTRSV_N_CLASSES][8] = {
+        // natural order / wavefront: SIMPLE 32 rows per task, STRIP one line per warp, WAVE 8 and 4 lines
+        // per CTA, and WAVE over 16 blocks with warm-ups (4 and 8 lines per CTA)
+        {SPTRSV_VAR_SIMPLE, 32, 8, 0, 0, 64, 4096, 0},   {SPTRSV_VAR_STRIP, 1, 2, 0, 0, 64, 4096, 0},
+        {SPTRSV_VAR_WAVE, 1, 8, 0, 0, 64, 4096, 0},      {SPTRSV_VAR_WAVE, 1, 4, 0, 0, 64, 4096, 0},
+        {SPTRSV_VAR_WAVE, 1, 4, 0, 0, 64, 4096, 16},     {SPTRSV_VAR_WAVE, 1, 8, 0, 0, 64, 4096, 16},
+        // ORDER: the reference's six tile sizes (analysis_csr.cu:84-102), 32..1 lanes per row
+        {SPTRSV_VAR_ORDER, 1, 8, 0, 0, 64, 4096, 0},     {SPTRSV_VAR_ORDER, 2, 8, 0, 0, 64, 4096, 0},
+        {SPTRSV_VAR_ORDER, 4, 8, 0, 0, 64, 4096, 0},     {SPTRSV_VAR_ORDER, 8, 8, 0, 0, 64, 4096, 0},
+        {SPTRSV_VAR_ORDER, 16, 8, 0, 0, 64, 4096, 0},    {SPTRSV_VAR_ORDER, 32, 8, 0, 0, 64, 4096, 0},
+        // MULTIROW over the reference's lane map: its own setting (class 12), back-off, fewer resident
+        // warps, 16-warp blocks, and over 16 and 128 blocks with warm-ups
+        {SPTRSV_VAR_MULTIROW, 1, 8, 0, 0, 64, 4096, 0},  {SPTRSV_VAR_MULTIROW, 1, 8, 0, 200, 64, 4096, 0},
+        {SPTRSV_VAR_MULTIROW, 1, 4, 16, 0, 64, 4096, 0}, {SPTRSV_VAR_MULTIROW, 1, 16, 0, 0, 64, 4096, 0},
+        {SPTRSV_VAR_MULTIROW, 1, 8, 0, 0, 64, 4096, 16}, {SPTRSV_VAR_MULTIROW, 1, 8, 0, 0, 64, 4096, 128},
+        // CLUSTER (bands of H levels cut into clusters of B rows) and BAND (one warp per unit), whole and
+        // over blocks with warm-ups
+        {SPTRSV_VAR_CLUSTER, 16, 16, 0, 0, 256, 2048, 0}, {SPTRSV_VAR_CLUSTER, 16, 8, 0, 0, 4096, 2048, 0},
+        {SPTRSV_VAR_BAND, 1, 8, 0, 0, 64, 4096, 0},       {SPTRSV_VAR_CLUSTER, 16, 16, 0, 0, 256, 2048, 16},
+        {SPTRSV_VAR_BAND, 1, 8, 0, 0, 64, 4096, 16},      {SPTRSV_VAR_BAND, 1, 8, 0, 0, 64, 4096, 128},
+    };
+    const int* t = T[cls];
+    s->variant = t[0];
+    s->rows_per_warp = t[1];
+    s->block_warps = t[2];
+    s->warps_per_sm = t[3];
+    s->backoff_ns = t[4];
     s->ir_max_iters = 2;
-    s->band_levels = 64;
-    s->cluster_rows = 4096;
-    s->partitions = 0;
-    if (v == SPTRSV_VAR_SIMPLE && nat_v[j] != SPTRSV_VAR_SIMPLE) {
-        s->variant = nat_v[j];
-        s->rows_per_warp = 1;
-        s->block_warps = nat_bw[j];
-    } else if (v == SPTRSV_VAR_SIMPLE || v == SPTRSV_VAR_ORDER) {
-        s->rows_per_warp = rpw[j];
-    } else if (v == SPTRSV_VAR_MULTIROW) {
-        s->block_warps = mr[j][0];
-        s->backoff_ns = mr[j][1];
-        s->warps_per_sm = mr[j][2];
-    } else {
-        s->band_levels = cl[j][0];
-        s->cluster_rows = cl[j][1];
-        s->rows_per_warp = cl[j][2];
-        s->block_warps = cl[j][3];
-    }
+    s->band_levels = t[5];
+    s->cluster_rows = t[6];
+    s->partitions = t[7];
     return ok();
 }
 

@@ -15,9 +15,12 @@ from . import _lib as C
 from ._lib import AnalysisInfo, Schedule, SpMat
 
 N_CLASSES = 24
+# version of the class table in csrc/tune.cu; weights trained on another
+# table are refused (their outputs would name other schedules)
+CLASS_TABLE = 2
 N_FEATURES = 12
 N_PARAMS = 6552
-VARIANT_NAMES = ["simple", "order", "multirow", "cluster", "strip", "wave"]
+VARIANT_NAMES = ["simple", "order", "multirow", "cluster", "strip", "wave", "band"]
 FEATURE_NAMES = ["log2_n", "log2_nnz", "nnz_per_row", "log2_nlevs", "log2_mean_level_width",
                  "log2_max_level_width", "q25_offdiag", "q50_offdiag", "q90_offdiag", "q99_offdiag",
                  "log2_1p_max_offdiag", "frac_diag_only"]
@@ -38,15 +41,18 @@ def schedule_from_class(cls: int) -> Schedule:
 def class_name(cls: int) -> str:
     s = schedule_from_class(cls)
     v = VARIANT_NAMES[s.variant]
+    part = f"-P{s.partitions}" if s.partitions >= 2 else ""
     if s.variant in (0, 1):
-        return f"{v}/rpw{s.rows_per_warp}"
+        return f"{v}/rpw{s.rows_per_warp}{part}"
     if s.variant == 4:
-        return f"{v}/R{s.rows_per_warp}-bw{s.block_warps}"
+        return f"{v}/R{s.rows_per_warp}-bw{s.block_warps}{part}"
     if s.variant == 5:
-        return f"{v}/G{s.block_warps}"
+        return f"{v}/G{s.block_warps}{part}"
+    if s.variant == 6:
+        return f"{v}{part}"
     if s.variant == 2:
-        return f"{v}/bw{s.block_warps}-bo{s.backoff_ns}-wps{s.warps_per_sm}"
-    return f"{v}/H{s.band_levels}-B{s.cluster_rows}-rpw{s.rows_per_warp}-bw{s.block_warps}"
+        return f"{v}/bw{s.block_warps}-bo{s.backoff_ns}-wps{s.warps_per_sm}{part}"
+    return f"{v}/H{s.band_levels}-B{s.cluster_rows}-rpw{s.rows_per_warp}-bw{s.block_warps}{part}"
 
 
 def autotune(plan, b, x, nrhs: int = 1, precision: int = 32, reps: int = 3):
@@ -129,11 +135,14 @@ class Mlp:
 
     def save(self, path):
         m, s = self.normalization()
-        np.savez(path, params=self.params(), mean=m, std=s)
+        np.savez(path, params=self.params(), mean=m, std=s, table=CLASS_TABLE)
 
     @classmethod
     def load(cls, path) -> "Mlp":
         z = np.load(path)
+        table = int(z["table"]) if "table" in z.files else 1
+        if table != CLASS_TABLE:
+            raise ValueError(f"{path}: weights for class table {table}, the library has table {CLASS_TABLE}")
         net = cls(0)
         net.set_params(z["params"])
         net.set_normalization(z["mean"], z["std"])

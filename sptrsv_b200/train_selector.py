@@ -11,9 +11,11 @@
    for the MLP, for the best single fixed class, and for the reference's own
    rule (its multirow solver, class 12), plus top-1 accuracy.
 
-Usage (GPU):  python -m sptrsv_b200.train_selector --n-train 500 --n-test 100 --out sptrsv_b200/selector
+Usage (GPU):  python -m sptrsv_b200.train_selector --n-train 2000 --n-test 400 --out sptrsv_b200/selector
 Writes <out>_data.npz (features, times, family, n), <out>_weights.npz and
-<out>_eval.json.
+<out>_eval.json.  The dataset can be collected in pieces (--collect-only
+--start S --count C --out <piece>, then --data <piece1>,<piece2>,... to
+train on their concatenation in matrix order).
 """
 from __future__ import annotations
 
@@ -54,7 +56,8 @@ def make_matrix(idx: int, seed: int, n_lo: int, n_hi: int):
     return fam, m
 
 
-def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print):
+def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print, start: int = 0):
+    """Matrices start .. start + n_total - 1 of the seeded sequence."""
     import torch
 
     import sptrsv_b200 as S
@@ -62,12 +65,12 @@ def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print)
 
     feats, times, fams, ns = [], [], [], []
     with ThreadPoolExecutor(max_workers=4) as ex:
-        futs = [ex.submit(make_matrix, i, seed, n_lo, n_hi) for i in range(min(n_total, 6))]
+        futs = [ex.submit(make_matrix, start + i, seed, n_lo, n_hi) for i in range(min(n_total, 6))]
         t0 = time.time()
         for i in range(n_total):
             fam, m = futs[i].result()
             if i + 6 < n_total:
-                futs.append(ex.submit(make_matrix, i + 6, seed, n_lo, n_hi))
+                futs.append(ex.submit(make_matrix, start + i + 6, seed, n_lo, n_hi))
             L = S.allocate_memory(m.rowptr, m.colidx, m.val, m.n)
             info = S.AnalysisInfo()
             info.mode = S.ALL
@@ -102,15 +105,19 @@ def evaluate(times: np.ndarray, choice: np.ndarray) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--n-train", type=int, default=500)
-    ap.add_argument("--n-test", type=int, default=100)
+    ap.add_argument("--n-train", type=int, default=2000)
+    ap.add_argument("--n-test", type=int, default=400)
     ap.add_argument("--n-lo", type=int, default=10_000)
-    ap.add_argument("--n-hi", type=int, default=2_000_000)
+    ap.add_argument("--n-hi", type=int, default=4_000_000)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--epochs", type=int, default=400)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--out", default="sptrsv_b200/selector")
-    ap.add_argument("--data", default=None, help="reuse a dataset npz instead of collecting")
+    ap.add_argument("--data", default=None,
+                    help="reuse dataset npz files (comma-separated pieces, concatenated) instead of collecting")
+    ap.add_argument("--collect-only", action="store_true", help="collect matrices start .. start+count-1 and stop")
+    ap.add_argument("--start", type=int, default=0)
+    ap.add_argument("--count", type=int, default=0)
     args = ap.parse_args()
 
     import torch
@@ -118,9 +125,19 @@ def main():
     from . import select as SEL
 
     torch.cuda.set_device(0)
+    if args.collect_only:
+        print(f"collecting matrices {args.start} .. {args.start + args.count - 1}", flush=True)
+        X, Tm, fam, ns = collect(args.count, args.seed, args.n_lo, args.n_hi, args.reps, start=args.start)
+        np.savez(f"{args.out}_data.npz", features=X, times=Tm, family=fam, n=ns, start=args.start)
+        return
     if args.data:
-        z = np.load(args.data)
-        X, Tm, fam, ns = z["features"], z["times"], z["family"], z["n"]
+        zs = [np.load(f) for f in args.data.split(",")]
+        zs.sort(key=lambda z: int(z["start"]) if "start" in z.files else 0)
+        X = np.concatenate([z["features"] for z in zs])
+        Tm = np.concatenate([z["times"] for z in zs])
+        fam = np.concatenate([z["family"] for z in zs])
+        ns = np.concatenate([z["n"] for z in zs])
+        np.savez(f"{args.out}_data.npz", features=X, times=Tm, family=fam, n=ns)
     else:
         print(f"collecting {args.n_train + args.n_test} matrices", flush=True)
         X, Tm, fam, ns = collect(args.n_train + args.n_test, args.seed, args.n_lo, args.n_hi, args.reps)

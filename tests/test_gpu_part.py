@@ -194,8 +194,8 @@ BAND_MATS = {
     "banded": lambda: gen.banded(30000, 256, 8, 8, seed=0),
     "banded_narrow": lambda: gen.banded(20000, 16, 4, 16, seed=11),
     "banded_var": lambda: gen.banded(9000, 64, 0, 24, seed=5),
-    "grid2d_small": lambda: gen.grid2d(40, 60, seed=1),
-    "chain": lambda: gen.banded(5000, 1, 1, 1, seed=2),
+    "grid2d_small": lambda: gen.grid2d(100, 70, seed=1),
+    "chain": lambda: gen.banded(8000, 1, 1, 1, seed=2),
 }
 
 
@@ -264,5 +264,30 @@ def test_band_refuses_wide_levels(torch_cuda):
     with pytest.raises(S.SptrsvError) as ei:
         plan.set_schedule(variant=S._lib.VAR_BAND)
     assert ei.value.code == -9
+    plan.close()
+    S.free_device_analysis(L, info)
+
+
+def test_partitioned_wave_streamed_host_solve(torch_cuda):
+    """Pinned host b and x with a partitioned WAVE plan: b is copied in
+    segments while the block system's kernel runs (warm-up rows read the
+    outer b), and each line group's real rows go straight to the host x."""
+    import sptrsv_b200 as S
+
+    torch = torch_cuda
+    m = gen.grid2d(600, 500, seed=7)
+    xt = gen.vector(m.n, "uniform", seed=8)
+    b = m.matvec(xt)
+    ref = O.solve(m.rowptr, m.colidx, m.val, b)
+    L, info = _setup(S, m)
+    plan = S.Plan(L, info)
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.zeros(m.n, dtype=torch.float64).pin_memory()
+    for P, G in ((16, 4), (5, 8)):
+        plan.set_schedule(variant=S._lib.VAR_WAVE, block_warps=G, partitions=P)
+        for _ in range(3):  # epochs advance from call to call
+            hx.zero_()
+            plan.solve_host(hb, hx, 1, precision=64)
+            assert O.rel_err(hx.numpy(), ref) <= TOL, (P, G)
     plan.close()
     S.free_device_analysis(L, info)
