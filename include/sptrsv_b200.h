@@ -288,6 +288,12 @@ int sptrsv_solve_f32(sptrsv_plan_t plan, const double* b, float* x32, int nrhs, 
 int sptrsv_solve_host(sptrsv_plan_t plan, const double* host_b, double* host_x, int nrhs,
                       int precision, cudaStream_t stream);
 
+/* Rows per segment of b in the streamed host solve (a multiple of 16; 0:
+ * the default, an eighth of the rows but at least 131072 = 1 MiB of
+ * doubles).  Fewer, larger segments mean fewer copies queued per solve; the
+ * kernel starts on the first segment once it has arrived. */
+int sptrsv_plan_set_stream_segment(sptrsv_plan_t plan, int rows);
+
 /* FP64 residual r = b - L x on the device (row-major n x nrhs). */
 int sptrsv_residual_f64(sptrsv_plan_t plan, const double* b, const double* x, double* r,
                         int nrhs, cudaStream_t stream);

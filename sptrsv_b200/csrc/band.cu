@@ -134,7 +134,20 @@ __global__ void k_band_gather(unsigned char* rec, const int* __restrict__ bidx, 
     }
 }
 
-// One step's record fields of this lane, in registers (U = 4).
+// One step's record pieces of this lane, as loaded (3-4 128-bit words), and
+// unpacked into the fields the step uses (U = 4).
+template <typename T>
+struct BandRaw {
+    static constexpr int NP = sizeof(T) == 8 ? 4 : 3;
+    uint4 c[NP];
+    __device__ __forceinline__ void fetch(const unsigned char* r, int lane)
+    {
+        const uint4* p = reinterpret_cast<const uint4*>(r) + lane;
+#pragma unroll
+        for (int k = 0; k < NP; k++) c[k] = p[32 * k];
+    }
+};
+
 template <typename T>
 struct BandStep {
     int kp, lend, os, xi;
@@ -151,33 +164,29 @@ struct BandStep {
         lend = (int)(c.z >> 24);
         xi = (int)c.w;
     }
-    __device__ __forceinline__ void load(const unsigned char* r, int lane);
+    __device__ __forceinline__ void unpack(const BandRaw<T>& r);
 };
 template <>
-__device__ __forceinline__ void BandStep<double>::load(const unsigned char* r, int lane)
+__device__ __forceinline__ void BandStep<double>::unpack(const BandRaw<double>& r)
 {
-    const uint4* p = reinterpret_cast<const uint4*>(r) + lane;
-    const uint4 c0 = p[0], c1 = p[32], c2 = p[64], c3 = p[96];
-    v[0] = __hiloint2double((int)c0.y, (int)c0.x);
-    v[1] = __hiloint2double((int)c0.w, (int)c0.z);
-    v[2] = __hiloint2double((int)c1.y, (int)c1.x);
-    v[3] = __hiloint2double((int)c1.w, (int)c1.z);
-    unpack_meta(c2);
-    inv = __hiloint2double((int)c3.y, (int)c3.x);
-    bv = __hiloint2double((int)c3.w, (int)c3.z);
+    v[0] = __hiloint2double((int)r.c[0].y, (int)r.c[0].x);
+    v[1] = __hiloint2double((int)r.c[0].w, (int)r.c[0].z);
+    v[2] = __hiloint2double((int)r.c[1].y, (int)r.c[1].x);
+    v[3] = __hiloint2double((int)r.c[1].w, (int)r.c[1].z);
+    unpack_meta(r.c[2]);
+    inv = __hiloint2double((int)r.c[3].y, (int)r.c[3].x);
+    bv = __hiloint2double((int)r.c[3].w, (int)r.c[3].z);
 }
 template <>
-__device__ __forceinline__ void BandStep<float>::load(const unsigned char* r, int lane)
+__device__ __forceinline__ void BandStep<float>::unpack(const BandRaw<float>& r)
 {
-    const uint4* p = reinterpret_cast<const uint4*>(r) + lane;
-    const uint4 c0 = p[0], c1 = p[32], c2 = p[64];
-    v[0] = __uint_as_float(c0.x);
-    v[1] = __uint_as_float(c0.y);
-    v[2] = __uint_as_float(c0.z);
-    v[3] = __uint_as_float(c0.w);
-    unpack_meta(c1);
-    inv = __uint_as_float(c2.x);
-    bv = __uint_as_float(c2.y);
+    v[0] = __uint_as_float(r.c[0].x);
+    v[1] = __uint_as_float(r.c[0].y);
+    v[2] = __uint_as_float(r.c[0].z);
+    v[3] = __uint_as_float(r.c[0].w);
+    unpack_meta(r.c[1]);
+    inv = __uint_as_float(r.c[2].x);
+    bv = __uint_as_float(r.c[2].y);
 }
 
 template <typename T, int U, int OUT>
@@ -188,10 +197,6 @@ __global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restr
     constexpr int rec_bytes = band_rec_bytes(sizeof(T));
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ __align__(8) unsigned long long bars[kBandNST];
-    // a chunk's results, written to x at the chunk's end: a global store
-    // between two levels would make the level barrier wait for it
-    __shared__ T outv[kBandCH * 32];
-    __shared__ int outi[kBandCH * 32];
     const int lane = threadIdx.x;
     T* ring = reinterpret_cast<T*>(sm);
     unsigned char* stage = sm + (((size_t)(R + 1) * sizeof(T) + 15) & ~(size_t)15);
@@ -239,44 +244,52 @@ __global__ void __launch_bounds__(32) k_sptrsv_band(const unsigned char* __restr
             }
             const unsigned char* cb = stage + k * chunk_bytes;
             const int steps = min(kBandCH, t1 - t0 - c * kBandCH);
-            // the record of step j + 1 is read into registers before step j
-            // touches the slots, so its loads are not held behind step j's
-            // shared-memory store (the compiler cannot tell the two apart)
+            // Per step, in issue order: the next record's loads, this step's
+            // slot loads, the next record's unpacking (its loads have landed by
+            // then), the sums, the slot store.  So the chain from one level's
+            // store to the next level's slot loads holds no other instruction.
+            // A chunk's results stay in registers and go to x after its last
+            // step, outside the level-to-level chain.
             BandStep<T> cur, nxt;
-            cur.load(cb, lane);
-            for (int j = 0; j < steps; j++) {
-                if (j + 1 < steps) nxt.load(cb + (size_t)(j + 1) * rec_bytes, lane);
-                // two partial sums halve the dependent multiply-add chain
-                T a0 = cur.bv, a1 = (T)0;
-#pragma unroll
-                for (int q = 0; q < U; q += 2) {
-                    a0 -= cur.v[q] * ring[cur.sl[q]];
-                    if (q + 1 < U) a1 -= cur.v[q + 1] * ring[cur.sl[q + 1]];
-                }
-                T acc = a0 + a1;
-                for (int o = cur.kp >> 1; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                int oi = -1;
-                if ((lane & (cur.kp - 1)) == 0 && cur.os < R) {
-                    const T xv = acc * cur.inv;
-                    ring[cur.os] = xv;
-                    outv[j * 32 + lane] = xv;
-                    oi = cur.xi;
-                }
-                outi[j * 32 + lane] = oi;
-                if (cur.lend) __syncwarp();
-                cur = nxt;
-            }
-            // the chunk's results to x (each lane its own slots of the buffer)
+            BandRaw<T> raw;
+            raw.fetch(cb, lane);
+            cur.unpack(raw);
+            T ov[kBandCH];
+            int oi[kBandCH];
 #pragma unroll
             for (int j = 0; j < kBandCH; j++) {
+                oi[j] = -1;
                 if (j < steps) {
-                    const int i = outi[j * 32 + lane];
-                    if (i >= 0) {
-                        const T v = outv[j * 32 + lane];
-                        if (x) x[i] = v;
-                        if (OUT == OUT_SET64) x64[i] = (double)v;
-                        if (OUT == OUT_ADD64) x64[i] += (double)v;
+                    if (j + 1 < steps) raw.fetch(cb + (size_t)(j + 1) * rec_bytes, lane);
+                    T rv[U];
+#pragma unroll
+                    for (int q = 0; q < U; q++) rv[q] = ring[cur.sl[q]];
+                    if (j + 1 < steps) nxt.unpack(raw);
+                    // two partial sums halve the dependent multiply-add chain
+                    T a0 = cur.bv, a1 = (T)0;
+#pragma unroll
+                    for (int q = 0; q < U; q += 2) {
+                        a0 -= cur.v[q] * rv[q];
+                        if (q + 1 < U) a1 -= cur.v[q + 1] * rv[q + 1];
                     }
+                    T acc = a0 + a1;
+                    for (int o = cur.kp >> 1; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                    if ((lane & (cur.kp - 1)) == 0 && cur.os < R) {
+                        const T xv = acc * cur.inv;
+                        ring[cur.os] = xv;
+                        ov[j] = xv;
+                        oi[j] = cur.xi;
+                    }
+                    if (cur.lend) __syncwarp();
+                    cur = nxt;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kBandCH; j++) {
+                if (oi[j] >= 0) {
+                    if (x) x[oi[j]] = ov[j];
+                    if (OUT == OUT_SET64) x64[oi[j]] = (double)ov[j];
+                    if (OUT == OUT_ADD64) x64[oi[j]] += (double)ov[j];
                 }
             }
             __syncwarp();

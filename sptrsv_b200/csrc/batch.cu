@@ -146,9 +146,9 @@ struct SeqSet {
 };
 
 constexpr int kVkU = 8;         // elements per wait round in the level-ordered kernel
-constexpr int kSeqRing = 1024;  // ring elements per sequential warp
+constexpr int kSeqRing = 2048;  // ring elements per sequential warp
 constexpr int kSeqEC = 512;     // entries of one 32-row chunk that fit a stage buffer
-constexpr int kSeqMaxK = 8;     // most right-hand sides one sequential warp carries (more: one warp per column)
+constexpr int kSeqMaxK = 32;    // most right-hand sides one sequential warp carries (lane q: column q)
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes_is8)
 {
@@ -337,17 +337,20 @@ __device__ __forceinline__ void seq_system(const SeqSet& q, const V* __restrict_
                             acc -= (T)sval[p] * __ldcg(x + off + (long long)(cc - r0) * K + lane);
                         }
                         const int msk = rw - 1;
+                        // four partial sums: the row's products are not one dependent chain
+                        T acc1 = 0, acc2 = 0, acc3 = 0;
                         for (; p + 4 <= e1; p += 4) {
                             const int c0 = scol[p], c1 = scol[p + 1], c2 = scol[p + 2], c3 = scol[p + 3];
                             const T v0 = (T)sval[p], v1 = (T)sval[p + 1], v2 = (T)sval[p + 2], v3 = (T)sval[p + 3];
                             const T x0 = rl[(c0 & msk) * kp], x1 = rl[(c1 & msk) * kp], x2 = rl[(c2 & msk) * kp],
                                     x3 = rl[(c3 & msk) * kp];
                             acc -= v0 * x0;
-                            acc -= v1 * x1;
-                            acc -= v2 * x2;
-                            acc -= v3 * x3;
+                            acc1 -= v1 * x1;
+                            acc2 -= v2 * x2;
+                            acc3 -= v3 * x3;
                         }
                         for (; p < e1; p++) acc -= (T)sval[p] * rl[(scol[p] & msk) * kp];
+                        acc += (acc1 + acc2) + acc3;
                     } else {
                         for (; p < e1; p++) {
                             const int cc = __ldg(gcol + p);

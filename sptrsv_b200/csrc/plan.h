@@ -160,6 +160,8 @@ struct sptrsv_plan_s {
     cudaEvent_t ev_start = nullptr, ev_copied = nullptr;
     const int* launch_bflag = nullptr;  // set only during a streamed launch
     int launch_epoch = 0;
+    int launch_seg_rows = 0;
+    int seg_rows = 0;            // rows per copied segment of b (0: the default, 1 MiB of doubles)
     double* launch_hx = nullptr;
     float* w32a = nullptr;
     float* w32b = nullptr;

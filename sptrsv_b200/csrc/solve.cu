@@ -19,9 +19,19 @@ bool pow2_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 
 
 // Rows of one WAVE line group: their FP64 x values fill the CTA's shared memory.
 constexpr int kWaveMaxRows = 200 * 1024 / 8;
-// Streamed host solves: rows per copied segment of b (1 MiB of doubles; a
-// multiple of 16 rows, so no 128-byte line of b spans two segments).
+// Streamed host solves: rows per copied segment of b, by default an eighth
+// of the rows but at least 131072 (1 MiB of doubles), a multiple of 16 rows
+// so no 128-byte line of b spans two segments; sptrsv_plan_set_stream_segment
+// sets a plan's own.  Every segment costs two queued copies (its rows and its
+// flag word), whose fixed cost outweighs an earlier start of the solve: on the
+// 2048 x 2048 grid 32 segments took 1.36 ms end to end, 8 segments 1.08 ms.
 constexpr int kStreamSegRows = 1 << 17;
+int stream_seg_rows(const sptrsv_plan_s* p)
+{
+    if (p->seg_rows > 0) return p->seg_rows;
+    const long long eighth = ((long long)p->n + 7) / 8;
+    return (int)std::max<long long>(kStreamSegRows, (eighth + 15) / 16 * 16);
+}
 
 // Shared memory of the STRIP kernel: per warp a ring of 2R chunks of 32 values.
 size_t strip_smem_bytes(const sptrsv_schedule_t* s, size_t elem)
@@ -205,7 +215,8 @@ void* mapped_host(const void* h)
 int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cudaStream_t s)
 {
     const int n = p->n;
-    const int nseg = (n + kStreamSegRows - 1) / kStreamSegRows;
+    const int seg_rows = stream_seg_rows(p);
+    const int nseg = (n + seg_rows - 1) / seg_rows;
     if (!p->bflag || p->nseg < nseg) {
         cudaFree(p->bflag);
         p->bflag = nullptr;
@@ -238,6 +249,7 @@ int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cuda
         xbuf = p->part->xx;
     }
     lp->launch_bflag = p->bflag;
+    lp->launch_seg_rows = seg_rows;
     lp->launch_epoch = p->epoch;
     lp->launch_hx = hx_dev;
     int e = plan_solve_f64(lp, p->hb, xbuf, 1, s);
@@ -245,7 +257,7 @@ int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cuda
     lp->launch_hx = nullptr;
     if (e) return e;
     for (int g = 0; g < nseg; g++) {
-        const size_t r0 = (size_t)g * kStreamSegRows, rows = std::min<size_t>(kStreamSegRows, n - r0);
+        const size_t r0 = (size_t)g * seg_rows, rows = std::min<size_t>(seg_rows, n - r0);
         SPT_CUDA(cudaMemcpyAsync(p->hb + r0, hb + r0, sizeof(double) * rows, cudaMemcpyHostToDevice,
                                  p->copy_stream));
         SPT_CUDA(cudaMemcpyAsync(p->bflag + g, p->epochs + p->epoch, sizeof(int), cudaMemcpyHostToDevice,
@@ -420,7 +432,7 @@ int plan_launch(sptrsv_plan_s* p, bool f32, const BT* b, T* x, double* x64, int 
         const size_t smem = (size_t)t.cap * sizeof(T);
         SPT_CUDA(allow_smem(kern, smem));
         SPT_CUDA(launch_persistent_capped(kern, block, smem, t.ngroups, cap, s, m, t.ngroups, b, x, x64, c->d_status,
-                                          budget, backoff, p->launch_bflag, kStreamSegRows, p->launch_epoch,
+                                          budget, backoff, p->launch_bflag, p->launch_seg_rows, p->launch_epoch,
                                           p->launch_hx));
         return 0;
     }
@@ -810,6 +822,17 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
         if (e) return e;
     }
     p->sched = *s;
+    return ok();
+}
+
+int sptrsv_plan_set_stream_segment(sptrsv_plan_t p, int rows)
+{
+    if (!p || rows < 0 || rows % 16 != 0)
+        return set_error(SPTRSV_ERR_INVALID_ARG, "set_stream_segment: rows must be 0 or a positive multiple of 16");
+    p->seg_rows = rows;
+    cudaFree(p->bflag);  // the flag words are sized by the segment count
+    p->bflag = nullptr;
+    p->nseg = 0;
     return ok();
 }
 

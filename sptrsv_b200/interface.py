@@ -200,6 +200,10 @@ class Plan:
     def update_values(self, gpu_L: SpMat):
         C.check(C.lib().sptrsv_plan_update_values(self._h, byref(gpu_L)))
 
+    def set_stream_segment(self, rows: int):
+        """Rows per copied segment of b in streamed host solves (0: default)."""
+        C.check(C.lib().sptrsv_plan_set_stream_segment(self._h, int(rows)))
+
     def partition_info(self) -> dict:
         """Blocks of a partitioned schedule: count, block-system rows, warm-up
         rows, truncation bound and the (s, a, e, base) table per block."""

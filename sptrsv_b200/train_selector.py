@@ -56,8 +56,9 @@ def make_matrix(idx: int, seed: int, n_lo: int, n_hi: int):
     return fam, m
 
 
-def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print, start: int = 0):
-    """Matrices start .. start + n_total - 1 of the seeded sequence."""
+def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print, start: int = 0, save=None):
+    """Matrices start .. start + n_total - 1 of the seeded sequence.  save(X,
+    T, fam, n), when given, is called every 25 matrices with what is done."""
     import torch
 
     import sptrsv_b200 as S
@@ -88,6 +89,9 @@ def collect(n_total: int, seed: int, n_lo: int, n_hi: int, reps: int, log=print,
             ns.append(m.n)
             if (i + 1) % 25 == 0:
                 log(f"  {i + 1}/{n_total} matrices ({time.time() - t0:.0f} s)")
+                if save:
+                    save(np.array(feats, np.float32), np.array(times, np.float32), np.array(fams, np.int32),
+                         np.array(ns, np.int64))
     return (np.array(feats, np.float32), np.array(times, np.float32), np.array(fams, np.int32),
             np.array(ns, np.int64))
 
@@ -127,8 +131,12 @@ def main():
     torch.cuda.set_device(0)
     if args.collect_only:
         print(f"collecting matrices {args.start} .. {args.start + args.count - 1}", flush=True)
-        X, Tm, fam, ns = collect(args.count, args.seed, args.n_lo, args.n_hi, args.reps, start=args.start)
-        np.savez(f"{args.out}_data.npz", features=X, times=Tm, family=fam, n=ns, start=args.start)
+        def save(X, Tm, fam, ns):
+            np.savez(f"{args.out}_data.npz", features=X, times=Tm, family=fam, n=ns, start=args.start)
+
+        X, Tm, fam, ns = collect(args.count, args.seed, args.n_lo, args.n_hi, args.reps, start=args.start,
+                                 save=save)
+        save(X, Tm, fam, ns)
         return
     if args.data:
         zs = [np.load(f) for f in args.data.split(",")]
@@ -143,6 +151,9 @@ def main():
         X, Tm, fam, ns = collect(args.n_train + args.n_test, args.seed, args.n_lo, args.n_hi, args.reps)
         np.savez(f"{args.out}_data.npz", features=X, times=Tm, family=fam, n=ns)
     ntr = args.n_train
+    if X.shape[0] < args.n_train + args.n_test:  # fewer matrices than asked for: 5/6 train, 1/6 held out
+        ntr = X.shape[0] * 5 // 6
+        print(f"{X.shape[0]} matrices: {ntr} train, {X.shape[0] - ntr} held out", flush=True)
     T, M = SEL.targets_from_times(Tm)
     net = SEL.Mlp(seed=args.seed)
     mean, std = X[:ntr].mean(0), X[:ntr].std(0)
