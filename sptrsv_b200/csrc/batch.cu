@@ -146,9 +146,9 @@ struct SeqSet {
 };
 
 constexpr int kVkU = 8;         // elements per wait round in the level-ordered kernel
-constexpr int kSeqRing = 2048;  // ring elements per sequential warp
+constexpr int kSeqRing = 1024;  // ring elements per sequential warp
 constexpr int kSeqEC = 512;     // entries of one 32-row chunk that fit a stage buffer
-constexpr int kSeqMaxK = 32;    // most right-hand sides one sequential warp carries (lane q: column q)
+constexpr int kSeqMaxK = 8;     // most right-hand sides one sequential warp carries (more: one warp per column)
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes_is8)
 {
