@@ -251,6 +251,11 @@ int sptrsv_plan_get_schedule(sptrsv_plan_t plan, sptrsv_schedule_t* s);
  * next block's a), first row in the block system. */
 int sptrsv_plan_partition_info(sptrsv_plan_t plan, int* blocks, int* n_ext, long long* warm_rows,
                                double* bound, int* table);
+/* The same blocks computed on the host from a host CSR, without a GPU
+ * (table: 4 ints per block as above; *bound the largest truncation bound).
+ * SPTRSV_ERR_UNSUPPORTED as for the schedule. */
+struct sptrsv_host_csr_s;
+int sptrsv_partition_blocks_host(const struct sptrsv_host_csr_s* m, int P, int* table, double* bound);
 /* Re-reads gpu_L->a (same pattern) into the plan's value copies. */
 int sptrsv_plan_update_values(sptrsv_plan_t plan, const sp_mat_t* gpu_L);
 
@@ -431,7 +436,7 @@ int sptrsv_plan_select_schedule(sptrsv_plan_t plan, sptrsv_mlp_t mlp, const sp_m
  * it.  These seeded generators make the benchmark matrices: square
  * lower-triangular CSR, sorted columns, diagonal last.  Arrays are malloc'd;
  * release them with sptrsv_host_csr_free. */
-typedef struct {
+typedef struct sptrsv_host_csr_s {
     int n;
     int nnz;
     int* rowptr;

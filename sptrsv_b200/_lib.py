@@ -99,6 +99,7 @@ _SIGS = {
     "sptrsv_plan_get_schedule": (c_int, [c_void_p, POINTER(Schedule)]),
     "sptrsv_plan_update_values": (c_int, [c_void_p, POINTER(SpMat)]),
     "sptrsv_plan_set_stream_segment": (c_int, [c_void_p, c_int]),
+    "sptrsv_partition_blocks_host": (c_int, [POINTER(HostCsr), c_int, c_void_p, POINTER(c_double)]),
     "sptrsv_plan_partition_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_longlong),
                                            POINTER(c_double), c_void_p]),
     "sptrsv_solve_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
