@@ -412,9 +412,7 @@ int build_part(sptrsv_plan_s* p, int P)
         std::swap(p->part, p->part_alt);
         return 0;
     }
-    part_delete(p->part_alt);
-    p->part_alt = p->part;
-    p->part = nullptr;
+    // built aside; the plan's block systems change only once this one is complete
     const int n = p->n;
     if (P < 2 || P > 4096) return set_error(SPTRSV_ERR_INVALID_ARG, "partitions: P must be in [2, 4096]");
     if ((long long)n < 256LL * P)  // blocks of fewer rows would be mostly warm-up
@@ -473,10 +471,8 @@ int build_part(sptrsv_plan_s* p, int P)
             }
         }
     }
-    p->part = q;
     auto fail = [&](int code) {
-        part_delete(p->part);
-        p->part = nullptr;
+        part_delete(q);
         return code;
     };
     e = allocate_memory(erp.data(), eci.data(), eva.data(), q->n_ext, &q->ext, ALL);
@@ -492,6 +488,9 @@ int build_part(sptrsv_plan_s* p, int P)
     if (cudaMalloc((void**)&q->d_tab, sizeof(int) * q->tab.size()) != cudaSuccess ||
         cudaMemcpy(q->d_tab, q->tab.data(), sizeof(int) * q->tab.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(cuda_fail(cudaGetLastError(), "partitions: block table"));
+    part_delete(p->part_alt);
+    p->part_alt = p->part;
+    p->part = q;
     return 0;
 }
 

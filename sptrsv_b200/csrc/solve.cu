@@ -797,13 +797,18 @@ int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
     int e = check_schedule(s);
     if (e) return e;
     if (s->partitions >= 2) {
-        // the variant runs on the block system
+        // the variant runs on the block system; if it cannot, the plan keeps
+        // the block system its current schedule uses
+        PartPlan* prev = p->part;
         e = build_part(p, s->partitions);
         if (e) return e;
         sptrsv_schedule_t inner = *s;
         inner.partitions = 0;
         e = sptrsv_plan_set_schedule(p->part->sub, &inner);
-        if (e) return e;
+        if (e) {
+            if (p->part != prev && p->part_alt == prev) std::swap(p->part, p->part_alt);
+            return e;
+        }
     } else if (s->variant == SPTRSV_VAR_CLUSTER) {
         e = build_cluster_layout(p, s->band_levels, s->cluster_rows);
         if (!e) e = build_cluster_tasks(p, s->rows_per_warp);
