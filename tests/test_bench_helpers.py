@@ -1,0 +1,52 @@
+"""bench.py's bookkeeping on the host: the launch count it claims per solve,
+the per-configuration summary it attaches to the headline, and the selector
+weights' class-table check (no GPU needed)."""
+import numpy as np
+
+import bench
+
+
+class _Sched:
+    def __init__(self, variant, partitions):
+        self.variant, self.partitions = variant, partitions
+
+
+def test_solve_launches_count_the_library_kernels():
+    # plain: one solve kernel; partitioned: gather, solve, scatter; BAND: b into the records, solve
+    assert bench.solve_launches(_Sched(5, 0), 64, 0) == 1
+    assert bench.solve_launches(_Sched(5, 16), 64, 0) == 3
+    assert bench.solve_launches(_Sched(6, 128), 64, 0) == 2
+    assert bench.solve_launches(_Sched(6, 0), 64, 0) == 2
+    # FP32 + refinement: a solve per step plus the first, and a residual per step
+    assert bench.solve_launches(_Sched(2, 0), 32, 1) == 1 * 2 + 1
+    assert bench.solve_launches(_Sched(5, 16), 32, 2) == 3 * 3 + 2
+
+
+def test_config_summary_keeps_the_figures_of_both_line_kinds():
+    single = {"config": {"workload": "w"}, "ms_per_step": 0.5, "value": 2000.0, "dtype": "f64", "steps": 10,
+              "schedule": {"name": "band-P128"}, "selected_by": "learned selector (MLP)",
+              "rel_err": {"tuned": 1e-15}, "gb_s": 25.0, "roofline": {"frac": 0.01, "achieved": 25.0},
+              "e2e": {"value": 1500.0}, "plain_fp64": {"ms": 5.0}, "speedup_vs_plain_fp64": 10.0,
+              "clocks": {"reasons": []}, "energy_j_per_solve": 0.1,
+              "cpu_baseline": {"value": 2000.0, "cores": 1, "kind": "port"},
+              "fp32_refine": {"ms": 0.9}, "fp64_tuned": {"ms": 0.5}}
+    out = bench.config_summary(single)
+    assert out["ms"] == 0.5 and out["solves_s"] == 2000.0 and out["fp32_refine_ms"] == 0.9
+    assert out["fp64_ms"] == 0.5 and out["cpu_ms_per_solve"] == 0.5 and out["e2e_solves_s"] == 1500.0
+    batch = dict(single, fp32_refine_best_ms=60.0, fp64_best_ms=30.0)
+    del batch["fp32_refine"], batch["fp64_tuned"]
+    out = bench.config_summary(batch)
+    assert out["fp32_refine_ms"] == 60.0 and out["fp64_ms"] == 30.0
+
+
+def test_selector_weights_of_another_class_table_are_refused(tmp_path, monkeypatch):
+    from sptrsv_b200 import select as SEL
+
+    w = tmp_path / "w.npz"
+    np.savez(w, params=np.zeros(SEL.N_PARAMS, np.float32), mean=np.zeros(12, np.float32),
+             std=np.ones(12, np.float32), table=SEL.CLASS_TABLE - 1)
+    monkeypatch.setattr(bench, "SELECTOR_WEIGHTS", w)
+    assert not bench.selector_ready(SEL)
+    np.savez(w, params=np.zeros(SEL.N_PARAMS, np.float32), mean=np.zeros(12, np.float32),
+             std=np.ones(12, np.float32), table=SEL.CLASS_TABLE)
+    assert bench.selector_ready(SEL)
