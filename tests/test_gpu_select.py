@@ -122,3 +122,61 @@ def test_autotune_picks_fastest_and_stays_correct(torch_cuda):
     net.close()
     plan.close()
     S.free_device_analysis(L, info)
+
+
+def test_selector_retrained_on_gpu_and_remeasured_live(torch_cuda):
+    """The shipped selector's data retrained from scratch by the CUDA forward,
+    backward and Adam kernels reaches a held-out regret close to the stored
+    evaluation's; then, on fresh matrices outside the data set, every class is
+    timed live and the learned choice is compared with the best class and
+    with the reference's own rule (its multirow solver for every matrix)."""
+    import json
+    from pathlib import Path
+
+    import sptrsv_b200 as S
+    from sptrsv_b200 import select as SEL
+    from sptrsv_b200 import train_selector as TS
+
+    torch = torch_cuda
+    pkg = Path(SEL.__file__).resolve().parent
+    if not (pkg / "selector_weights.npz").exists():
+        pytest.skip("selector not trained")
+    d = np.load(pkg / "selector_data.npz")
+    ev = json.loads((pkg / "selector_eval.json").read_text())
+    X, Tm = d["features"], d["times"]
+    ntr = ev["n_train"]
+    T, M = SEL.targets_from_times(Tm)
+    net = SEL.Mlp(seed=11)
+    mean, std = X[:ntr].mean(0), X[:ntr].std(0)
+    net.set_normalization(mean, np.where(std > 1e-6, std, 1.0).astype(np.float32))
+    curve = net.train(X[:ntr], T[:ntr], M[:ntr], epochs=400, batch=64, lr=2e-3, seed=11)
+    assert curve[-1] < 0.5 * curve[0]
+    Y = net.forward(X[ntr:])
+    Y[~np.isfinite(Tm[ntr:])] = np.inf
+    held_out = TS.evaluate(Tm[ntr:], Y.argmin(axis=1))
+    assert held_out["mean_regret"] <= ev["mlp"]["test"]["mean_regret"] + 0.10, held_out
+    assert held_out["geomean_time_over_best"] <= 1.1, held_out
+    net.close()
+    # live: fresh matrices (seeds and sizes not in the data set), every class timed
+    shipped = SEL.Mlp.load(pkg / "selector_weights.npz")
+    ratios_best, ratios_ref = [], []
+    for m in (gen.banded(60000, 96, 4, 12, seed=901), gen.grid2d(320, 260, seed=902), gen.grid3d(36, 36, 36, seed=903),
+              gen.zipf(80000, 1.5, 256, seed=904)):
+        L, info = _setup(S, m)
+        plan = S.Plan(L, info)
+        b = torch.from_numpy(m.matvec(gen.vector(m.n, "uniform", seed=905))).cuda()
+        x = torch.empty_like(b)
+        _, times = SEL.autotune(plan, b, x, 1, 64, reps=3)
+        cls = shipped.select(plan, L, info)
+        plan.solve_f64(b, x)
+        S.sync_status()
+        assert O.rel_err(x.cpu().numpy(), O.solve(m.rowptr, m.colidx, m.val, b.cpu().numpy())) <= 1e-12
+        ratios_best.append(float(times[cls] / np.nanmin(times)))
+        ratios_ref.append(float(times[12] / times[cls]))
+        plan.close()
+        S.free_device_analysis(L, info)
+    shipped.close()
+    gm = lambda v: float(np.exp(np.mean(np.log(v))))  # noqa: E731
+    # the learned choice is close to the exhaustive autotuner's and ahead of the reference's rule
+    assert gm(ratios_best) <= 1.5, ratios_best
+    assert gm(ratios_ref) >= 1.1, ratios_ref
