@@ -221,7 +221,9 @@ int solve_host_streamed(sptrsv_plan_s* p, const double* hb, double* hx_dev, cuda
         cudaFree(p->bflag);
         p->bflag = nullptr;
         SPT_CUDA(dalloc(&p->bflag, nseg));
-        SPT_CUDA(cudaMemset(p->bflag, 0, sizeof(int) * (size_t)nseg));
+        // zeroed on s, which the copy stream follows (a legacy-stream memset
+        // is not ordered before work on a non-blocking stream)
+        SPT_CUDA(cudaMemsetAsync(p->bflag, 0, sizeof(int) * (size_t)nseg, s));
         p->nseg = nseg;
     }
     if (!p->epochs) {
