@@ -812,7 +812,8 @@ def run_batch(args, rank, world, local, dist):
     apply(best)
     achieved = nbytes / (t64 / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": load_traffic("batch_f64_c3"), "kernel": "k_sptrsv_vk (one FP64 launch per solve)",
+                "traffic": load_traffic(f"batch{f'_p{c64[0]}' if c64[0] else ''}_f64_c3"),
+                "kernel": "k_sptrsv_vk (one FP64 launch per solve)",
                 "algorithmic_bytes_per_launch": nbytes, "launch_ms": t64, "peak_kind": peak_kind,
                 "union_levels": batch.nlevs}
 
