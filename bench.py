@@ -727,11 +727,11 @@ def run_batch(args, rank, world, local, dist):
         flush_buf.fill_(1)
 
     if args.lean:
-        # profiling run: the default hybrid schedule, warm-up and the timed solves, nothing else
+        # profiling run: one schedule (--batch-mode/--batch-width/--batch-bw), warm-up and the timed solves
         prec = args.lean
         batch.set_partition(args.part)
-        batch.set_seq_width(16.0)
-        batch.set_schedule(mode=2, block_warps=4, ir_iters=1 if prec == 32 else 0)
+        batch.set_seq_width(args.batch_width)
+        batch.set_schedule(mode=args.batch_mode, block_warps=args.batch_bw, ir_iters=1 if prec == 32 else 0)
         ts = event_time_steps(torch, lambda: batch.solve_graph(db, dx, prec), args.steps, args.warmup, flush, stream)
         S.sync_status()
         print(json.dumps({"lean": True, "systems": len(mats), "precision": prec, "ms_per_step": sum(ts) / len(ts)}),
@@ -937,6 +937,12 @@ def main():
                     help="profiling runs (--lean) of c3 only: cut long systems into blocks of about this many rows")
     ap.add_argument("--systems", type=int, default=512,
                     help="profiling runs (--lean) of c3 only: the number of systems in the batch")
+    ap.add_argument("--batch-mode", type=int, default=2, choices=[0, 1, 2],
+                    help="profiling runs (--lean) of c3 only: 0 level order, 1 natural-order chunks, 2 hybrid")
+    ap.add_argument("--batch-width", type=float, default=16.0,
+                    help="profiling runs (--lean) of c3 only: the hybrid's mean-level-width threshold")
+    ap.add_argument("--batch-bw", type=int, default=4,
+                    help="profiling runs (--lean) of c3 only: warps per block")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
