@@ -901,7 +901,7 @@ def config_summary(line: dict) -> dict:
         "workload": line["config"]["workload"], "config": line["config"], "ms": line["ms_per_step"],
         "solves_s": line["value"], "dtype": line["dtype"], "steps": line["steps"], "schedule": line.get("schedule"),
         "selected_by": line.get("selected_by"), "rel_err": line["rel_err"], "gb_s": line.get("gb_s"),
-        "roofline": {k: rf.get(k) for k in ("achieved", "peak", "frac", "unit", "kernel", "launch_ms")},
+        "roofline": {k: rf.get(k) for k in ("achieved", "peak", "frac", "unit", "traffic", "kernel", "launch_ms")},
         "e2e_solves_s": line["e2e"]["value"], "plain_fp64": line.get("plain_fp64"),
         "speedup_vs_plain_fp64": line.get("speedup_vs_plain_fp64"), "clocks": line.get("clocks"),
         "energy_j_per_solve": line.get("energy_j_per_solve"),

@@ -25,7 +25,8 @@ def test_solve_launches_count_the_library_kernels():
 def test_config_summary_keeps_the_figures_of_both_line_kinds():
     single = {"config": {"workload": "w"}, "ms_per_step": 0.5, "value": 2000.0, "dtype": "f64", "steps": 10,
               "schedule": {"name": "band-P128"}, "selected_by": "learned selector (MLP)",
-              "rel_err": {"tuned": 1e-15}, "gb_s": 25.0, "roofline": {"frac": 0.01, "achieved": 25.0},
+              "rel_err": {"tuned": 1e-15}, "gb_s": 25.0,
+              "roofline": {"frac": 0.01, "achieved": 25.0, "traffic": 178495488},
               "e2e": {"value": 1500.0}, "plain_fp64": {"ms": 5.0}, "speedup_vs_plain_fp64": 10.0,
               "clocks": {"reasons": []}, "energy_j_per_solve": 0.1,
               "cpu_baseline": {"value": 2000.0, "cores": 1, "kind": "port"},
@@ -33,6 +34,7 @@ def test_config_summary_keeps_the_figures_of_both_line_kinds():
     out = bench.config_summary(single)
     assert out["ms"] == 0.5 and out["solves_s"] == 2000.0 and out["fp32_refine_ms"] == 0.9
     assert out["fp64_ms"] == 0.5 and out["cpu_ms_per_solve"] == 0.5 and out["e2e_solves_s"] == 1500.0
+    assert out["roofline"]["traffic"] == 178495488 and out["roofline"]["frac"] == 0.01
     batch = dict(single, fp32_refine_best_ms=60.0, fp64_best_ms=30.0)
     del batch["fp32_refine"], batch["fp64_tuned"]
     out = bench.config_summary(batch)
@@ -50,3 +52,11 @@ def test_selector_weights_of_another_class_table_are_refused(tmp_path, monkeypat
     np.savez(w, params=np.zeros(SEL.N_PARAMS, np.float32), mean=np.zeros(12, np.float32),
              std=np.ones(12, np.float32), table=SEL.CLASS_TABLE)
     assert bench.selector_ready(SEL)
+
+
+def test_traffic_of_every_bench_schedule_is_on_record():
+    # the schedules the default run picks: WAVE over 16 blocks (grid), BAND over 128 blocks (banded),
+    # the multi-RHS kernel (Zipf, 16 RHS), the batch cut into blocks of 4096 rows
+    for key in ("wave_p16_f64_c1", "band_p128_f64_c0", "multirow_f64_c2k16", "batch_p4096_f64_c3"):
+        t = bench.load_traffic(key)
+        assert isinstance(t, int) and t > 0, key
