@@ -121,3 +121,77 @@ def test_generator_shapes_match_configs():
     assert offs.max() <= 256 and 0.30 < np.mean(offs == 0) < 0.45  # P(Z=1) = 1/zeta(1.5) = 0.383
     bd = gen.blockdiag(96, 32)
     assert np.array_equal(np.diff(bd.rowptr) - 1, np.tile(np.arange(32), 3))
+
+
+_NULL_CALLS = """
+import ctypes, json
+from sptrsv_b200 import _lib as C
+L = C.lib()
+p = ctypes.c_void_p(0)
+calls = [
+    ("sptrsv_plan_create", (None, None, ctypes.byref(p))),
+    ("sptrsv_plan_set_schedule", (None, None)),
+    ("sptrsv_plan_get_schedule", (None, None)),
+    ("sptrsv_plan_partition_info", (None, None, None, None, None, None)),
+    ("sptrsv_partition_blocks_host", (None, 16, None, None)),
+    ("sptrsv_plan_update_values", (None, None)),
+    ("sptrsv_solve_f64", (None, None, None, 1, None)),
+    ("sptrsv_solve_ir", (None, None, None, 1, None)),
+    ("sptrsv_solve_f32", (None, None, None, 1, None)),
+    ("sptrsv_plan_calibrate_ir", (None, None, None, 1, 1e-12, 4, None, None)),
+    ("sptrsv_solve_host", (None, None, None, 1, 64, None)),
+    ("sptrsv_plan_set_stream_segment", (None, 16)),
+    ("sptrsv_residual_f64", (None, None, None, None, 1, None)),
+    ("sptrsv_solve_ir_noalloc", (None, None, None, 1, None)),
+    ("sptrsv_batch_create", (0, None, None, ctypes.byref(p))),
+    ("sptrsv_batch_info", (None, None, None, None, None)),
+    ("sptrsv_batch_set_schedule", (None, 0, 8, 0, 0, 0)),
+    ("sptrsv_batch_set_seq_width", (None, 16.0)),
+    ("sptrsv_batch_seq_systems", (None, None, None, None)),
+    ("sptrsv_batch_set_partition", (None, 4096)),
+    ("sptrsv_batch_partition_info", (None, None, None, None, None)),
+    ("sptrsv_batch_solve", (None, None, None, 64, None)),
+    ("sptrsv_batch_solve_graph", (None, None, None, 64, None)),
+    ("sptrsv_features", (None, None, None)),
+    ("sptrsv_schedule_from_class", (-1, None)),
+    ("sptrsv_autotune", (None, None, None, 1, 64, 3, None, None)),
+    ("sptrsv_mlp_get_params", (None, None)),
+    ("sptrsv_mlp_set_params", (None, None)),
+    ("sptrsv_mlp_set_normalization", (None, None, None)),
+    ("sptrsv_mlp_get_normalization", (None, None, None)),
+    ("sptrsv_mlp_forward_host", (None, None, 1, None)),
+    ("sptrsv_mlp_gradient_host", (None, None, None, None, 1, None, None)),
+    ("sptrsv_mlp_train_host", (None, None, None, None, 1, 1, 1, 1e-3, 0, None)),
+    ("sptrsv_mlp_predict_class", (None, None, None)),
+    ("sptrsv_plan_select_schedule", (None, None, None, None, None)),
+    ("sptrsv_solve_order_tile", (None, None, None, None, 1, None)),
+    ("sptrsv_host_spmv", (None, None, None, 1)),
+    ("sptrsv_read_mtx_lower", (None, 0, None)),
+    ("sptrsv_analysis_levels", (None, None)),
+    ("sptrsv_analysis_buckets", (None, None)),
+    ("sptrsv_plan_destroy", (None,)),
+    ("sptrsv_batch_destroy", (None,)),
+    ("sptrsv_mlp_destroy", (None,)),
+]
+print(json.dumps({name: getattr(L, name)(*args) for name, args in calls}))
+"""
+
+
+def test_null_handles_and_arguments_are_refused_without_a_crash():
+    """Every entry point given NULL handles or buffers returns an error code
+    (NULL is fine for the destroy functions) instead of dereferencing them;
+    the calls run in a child process, so a crash fails this test."""
+    import json
+    import subprocess
+    import sys
+
+    r = subprocess.run([sys.executable, "-c", _NULL_CALLS], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    codes = json.loads(r.stdout.strip().splitlines()[-1])
+    for name, code in codes.items():
+        if name.endswith("_destroy"):
+            assert code == 0, name
+        elif name.startswith("sptrsv_analysis_"):
+            assert code == -6, (name, code)  # SPTRSV_ERR_NOT_ANALYSED
+        else:
+            assert code == -2, (name, code)  # SPTRSV_ERR_INVALID_ARG
