@@ -98,3 +98,75 @@ def test_rejects_bad_files(tmp_path):
         gen.read_mtx_lower(p)
     with pytest.raises(SptrsvError):
         gen.read_mtx_lower(tmp_path / "missing.mtx")
+
+
+def test_long_lines_and_an_inflated_entry_count(tmp_path):
+    p = tmp_path / "long.mtx"
+    # a comment longer than any fixed line buffer is still one comment
+    _write(p, "%%MatrixMarket matrix coordinate real general", 3, [(1, 1, 2.0), (2, 1, -1.0), (2, 2, 4.0), (3, 3, 5.0)],
+           comments=("%" + "x" * 20000,))
+    m = gen.read_mtx_lower(p, unit_values=False)
+    assert m.n == 3 and np.allclose(_to_dense(m), [[2, 0, 0], [-1, 4, 0], [0, 0, 5]])
+    # a size line claiming far more entries than the file holds is refused, not allocated for
+    p.write_text("%%MatrixMarket matrix coordinate real general\n3 3 999999999999\n1 1 1.0\n")
+    with pytest.raises(SptrsvError):
+        gen.read_mtx_lower(p)
+
+
+_FUZZ = r"""
+import ctypes, json, sys
+import numpy as np
+from sptrsv_b200 import _lib as C
+rng = np.random.default_rng(7)
+d = sys.argv[1]
+tokens = ["%%MatrixMarket", "matrix", "coordinate", "real", "pattern", "integer", "general", "symmetric",
+          "skew-symmetric", "%", "1", "2", "3", "0", "-1", "4", "1e300", "nan", "x", "", "\t", "99999999999"]
+codes = []
+for t in range(300):
+    if t % 3 == 0:  # a valid file, then perhaps one line replaced by shuffled tokens
+        n = int(rng.integers(1, 6))
+        ent = [(int(rng.integers(1, n + 1)), int(rng.integers(1, n + 1)), float(rng.normal())) for _ in range(6)]
+        lines = ["%%MatrixMarket matrix coordinate real " + str(rng.choice(["general", "symmetric"])),
+                 f"{n} {n} {len(ent)}"] + [f"{i} {j} {v}" for i, j, v in ent]
+        if rng.random() < 0.5:
+            lines[int(rng.integers(0, len(lines)))] = " ".join(rng.choice(tokens, size=rng.integers(0, 5)))
+    else:
+        lines = ["%%MatrixMarket matrix coordinate real general" if rng.random() < 0.7 else
+                 " ".join(rng.choice(tokens, size=rng.integers(1, 6)))]
+        for _ in range(int(rng.integers(0, 8))):
+            lines.append(" ".join(rng.choice(tokens, size=rng.integers(0, 5))))
+    path = f"{d}/f{t}.mtx"
+    data = "\n".join(lines)
+    if rng.random() < 0.2:  # raw bytes, NULs included
+        data = rng.integers(0, 256, size=int(rng.integers(1, 400)), dtype=np.uint8).tobytes().decode("latin-1")
+    open(path, "w", encoding="latin-1").write(data)
+    m = C.HostCsr()
+    r = C.lib().sptrsv_read_mtx_lower(path.encode(), 0, ctypes.byref(m))
+    ok = True
+    if r == 0:
+        bad = ctypes.c_int(-1)
+        ok = C.lib().sptrsv_check_csr_host(m.rowptr, m.colidx, m.n, ctypes.byref(bad)) == 0
+        C.lib().sptrsv_host_csr_free(ctypes.byref(m))
+    codes.append([int(r), bool(ok)])
+print(json.dumps(codes))
+"""
+
+
+def test_garbage_files_give_an_error_or_a_valid_matrix(tmp_path):
+    """Seeded random files (plausible lines, shuffled tokens, raw bytes) read in
+    a child process: each gives an error code or a lower-triangular CSR with
+    the diagonal last, and none crashes the reader."""
+    import json
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    r = subprocess.run([sys.executable, "-c", _FUZZ, str(tmp_path)], cwd=ROOT, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    codes = json.loads(r.stdout.strip().splitlines()[-1])
+    assert len(codes) == 300
+    assert all(code in (0, -2, -7, -9) for code, _ in codes)
+    assert all(ok for code, ok in codes if code == 0)
+    assert any(code == 0 for code, _ in codes) and any(code == -2 for code, _ in codes)
