@@ -105,8 +105,10 @@ int compute_features(const sp_mat_t* L, const dfr_analysis_info_t* info, float* 
 
 extern "C" int sptrsv_features(const sp_mat_t* L, const dfr_analysis_info_t* info, float* out12)
 {
-    if (!L || !info || !out12) return sptrsv::set_error(SPTRSV_ERR_INVALID_ARG, "features: NULL argument");
-    if (!info->iorder) return sptrsv::set_error(SPTRSV_ERR_NOT_ANALYSED, "features: info is not analysed");
-    int e = sptrsv::compute_features(L, info, out12);
-    return e ? e : sptrsv::ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!L || !info || !out12) return sptrsv::set_error(SPTRSV_ERR_INVALID_ARG, "features: NULL argument");
+        if (!info->iorder) return sptrsv::set_error(SPTRSV_ERR_NOT_ANALYSED, "features: info is not analysed");
+        int e = sptrsv::compute_features(L, info, out12);
+        return e ? e : sptrsv::ok();
+    });
 }

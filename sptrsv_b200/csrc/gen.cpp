@@ -123,7 +123,10 @@ struct Builder {
         out->rowptr = (int*)malloc(sizeof(int) * rowptr.size());
         out->colidx = (int*)malloc(sizeof(int) * (col.size() ? col.size() : 1));
         out->val = (double*)malloc(sizeof(double) * (val.size() ? val.size() : 1));
-        if (!out->rowptr || !out->colidx || !out->val) return SPTRSV_ERR_ALLOC;
+        if (!out->rowptr || !out->colidx || !out->val) {
+            sptrsv_host_csr_free(out);
+            return SPTRSV_ERR_ALLOC;
+        }
         memcpy(out->rowptr, rowptr.data(), sizeof(int) * rowptr.size());
         if (!col.empty()) memcpy(out->colidx, col.data(), sizeof(int) * col.size());
         if (!val.empty()) memcpy(out->val, val.data(), sizeof(double) * val.size());
@@ -131,135 +134,157 @@ struct Builder {
     }
 };
 
+// No C++ exception leaves the C ABI: host memory that cannot be had (a
+// huge n, a corrupt size) is SPTRSV_ERR_ALLOC.
+template <class F>
+int host_guard(F&& f) noexcept
+{
+    try {
+        return f();
+    } catch (...) {
+        return SPTRSV_ERR_ALLOC;
+    }
+}
+
 }  // namespace
 
 extern "C" {
 
 int sptrsv_gen_banded(int n, int bandwidth, int off_min, int off_max, uint64_t seed, sptrsv_host_csr_t* out)
 {
-    if (!out || n < 0 || bandwidth < 1 || off_min < 0 || off_max < off_min) return SPTRSV_ERR_INVALID_ARG;
-    memset(out, 0, sizeof(*out));
-    Rng g(seed);
-    DistinctSampler ds;
-    Builder b;
-    b.col.reserve((size_t)n * (off_max + 1));
-    b.val.reserve((size_t)n * (off_max + 1));
-    std::vector<int> cols;
-    for (int i = 0; i < n; i++) {
-        int k = off_min == off_max ? off_min : off_min + (int)g.below((uint64_t)(off_max - off_min + 1));
-        int lo = std::max(0, i - bandwidth);
-        k = std::min(k, i - lo);
-        ds.sample(g, lo, i, k, cols);
-        b.row_dominant(g, i, cols);
-    }
-    return b.finish(out);
+    return host_guard([&]() -> int {
+        if (!out || n < 0 || bandwidth < 1 || off_min < 0 || off_max < off_min) return SPTRSV_ERR_INVALID_ARG;
+        memset(out, 0, sizeof(*out));
+        Rng g(seed);
+        DistinctSampler ds;
+        Builder b;
+        b.col.reserve((size_t)n * (off_max + 1));
+        b.val.reserve((size_t)n * (off_max + 1));
+        std::vector<int> cols;
+        for (int i = 0; i < n; i++) {
+            int k = off_min == off_max ? off_min : off_min + (int)g.below((uint64_t)(off_max - off_min + 1));
+            int lo = std::max(0, i - bandwidth);
+            k = std::min(k, i - lo);
+            ds.sample(g, lo, i, k, cols);
+            b.row_dominant(g, i, cols);
+        }
+        return b.finish(out);
+    });
 }
 
 int sptrsv_gen_grid2d(int nx, int ny, uint64_t seed, sptrsv_host_csr_t* out)
 {
-    if (!out || nx < 1 || ny < 1 || (long long)nx * ny > 0x7fffffffLL / 3) return SPTRSV_ERR_INVALID_ARG;
-    memset(out, 0, sizeof(*out));
-    Rng g(seed);
-    Builder b;
-    long long n = (long long)nx * ny;
-    b.col.reserve((size_t)n * 3);
-    b.val.reserve((size_t)n * 3);
-    for (int r = 0; r < ny; r++)
-        for (int c = 0; c < nx; c++) {
-            int i = r * nx + c;
-            if (r > 0) {
-                b.col.push_back(i - nx);
-                b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
-            }
-            if (c > 0) {
-                b.col.push_back(i - 1);
-                b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
-            }
-            b.col.push_back(i);
-            b.val.push_back(4.0);
-            b.rowptr.push_back((int)b.col.size());
-        }
-    return b.finish(out);
-}
-
-int sptrsv_gen_grid3d(int nx, int ny, int nz, uint64_t seed, sptrsv_host_csr_t* out)
-{
-    if (!out || nx < 1 || ny < 1 || nz < 1 || (long long)nx * ny * nz > 0x7fffffffLL / 4) return SPTRSV_ERR_INVALID_ARG;
-    memset(out, 0, sizeof(*out));
-    Rng g(seed);
-    Builder b;
-    for (int z = 0; z < nz; z++)
-        for (int y = 0; y < ny; y++)
-            for (int x = 0; x < nx; x++) {
-                int i = (z * ny + y) * nx + x;
-                if (z > 0) {
-                    b.col.push_back(i - nx * ny);
-                    b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
-                }
-                if (y > 0) {
+    return host_guard([&]() -> int {
+        if (!out || nx < 1 || ny < 1 || (long long)nx * ny > 0x7fffffffLL / 3) return SPTRSV_ERR_INVALID_ARG;
+        memset(out, 0, sizeof(*out));
+        Rng g(seed);
+        Builder b;
+        long long n = (long long)nx * ny;
+        b.col.reserve((size_t)n * 3);
+        b.val.reserve((size_t)n * 3);
+        for (int r = 0; r < ny; r++)
+            for (int c = 0; c < nx; c++) {
+                int i = r * nx + c;
+                if (r > 0) {
                     b.col.push_back(i - nx);
                     b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
                 }
-                if (x > 0) {
+                if (c > 0) {
                     b.col.push_back(i - 1);
                     b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
                 }
                 b.col.push_back(i);
-                b.val.push_back(6.0);
+                b.val.push_back(4.0);
                 b.rowptr.push_back((int)b.col.size());
             }
-    return b.finish(out);
+        return b.finish(out);
+    });
+}
+
+int sptrsv_gen_grid3d(int nx, int ny, int nz, uint64_t seed, sptrsv_host_csr_t* out)
+{
+    return host_guard([&]() -> int {
+        if (!out || nx < 1 || ny < 1 || nz < 1 || (long long)nx * ny * nz > 0x7fffffffLL / 4) return SPTRSV_ERR_INVALID_ARG;
+        memset(out, 0, sizeof(*out));
+        Rng g(seed);
+        Builder b;
+        for (int z = 0; z < nz; z++)
+            for (int y = 0; y < ny; y++)
+                for (int x = 0; x < nx; x++) {
+                    int i = (z * ny + y) * nx + x;
+                    if (z > 0) {
+                        b.col.push_back(i - nx * ny);
+                        b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
+                    }
+                    if (y > 0) {
+                        b.col.push_back(i - nx);
+                        b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
+                    }
+                    if (x > 0) {
+                        b.col.push_back(i - 1);
+                        b.val.push_back(-1.0 + g.uniform(-0.1, 0.1));
+                    }
+                    b.col.push_back(i);
+                    b.val.push_back(6.0);
+                    b.rowptr.push_back((int)b.col.size());
+                }
+        return b.finish(out);
+    });
 }
 
 // Off-diagonal count per row = min(Z - 1, max_off, i) with Z ~ Zipf(s) on
 // {1, 2, ...}; columns distinct, uniform over all preceding rows.
 int sptrsv_gen_zipf(int n, double s, int max_off, uint64_t seed, sptrsv_host_csr_t* out)
 {
-    if (!out || n < 0 || s <= 1.0 || max_off < 0) return SPTRSV_ERR_INVALID_ARG;
-    memset(out, 0, sizeof(*out));
-    // zeta(s) by a long partial sum plus the Euler-Maclaurin tail
-    const int N = 1000000;
-    double zeta = 0.0;
-    for (int k = N; k >= 1; k--) zeta += std::pow((double)k, -s);
-    zeta += std::pow((double)N, 1.0 - s) / (s - 1.0) - 0.5 * std::pow((double)N, -s);
-    std::vector<double> cdf(max_off > 0 ? max_off : 1);
-    double acc = 0.0;
-    for (int k = 1; k <= max_off; k++) {  // P(count = k-1) = P(Z = k)
-        acc += std::pow((double)k, -s) / zeta;
-        cdf[k - 1] = acc;
-    }
-    Rng g(seed);
-    DistinctSampler ds;
-    Builder b;
-    std::vector<int> cols;
-    for (int i = 0; i < n; i++) {
-        double u = g.u01();
-        int cnt = max_off;
-        if (max_off > 0) {
-            auto it = std::lower_bound(cdf.begin(), cdf.end(), u);
-            if (it != cdf.end()) cnt = (int)(it - cdf.begin());
+    return host_guard([&]() -> int {
+        if (!out || n < 0 || s <= 1.0 || max_off < 0) return SPTRSV_ERR_INVALID_ARG;
+        memset(out, 0, sizeof(*out));
+        // zeta(s) by a long partial sum plus the Euler-Maclaurin tail
+        const int N = 1000000;
+        double zeta = 0.0;
+        for (int k = N; k >= 1; k--) zeta += std::pow((double)k, -s);
+        zeta += std::pow((double)N, 1.0 - s) / (s - 1.0) - 0.5 * std::pow((double)N, -s);
+        std::vector<double> cdf(max_off > 0 ? max_off : 1);
+        double acc = 0.0;
+        for (int k = 1; k <= max_off; k++) {  // P(count = k-1) = P(Z = k)
+            acc += std::pow((double)k, -s) / zeta;
+            cdf[k - 1] = acc;
         }
-        cnt = std::min(cnt, i);
-        ds.sample(g, 0, i, cnt, cols);
-        b.row_dominant(g, i, cols);
-    }
-    return b.finish(out);
+        Rng g(seed);
+        DistinctSampler ds;
+        Builder b;
+        std::vector<int> cols;
+        for (int i = 0; i < n; i++) {
+            double u = g.u01();
+            int cnt = max_off;
+            if (max_off > 0) {
+                auto it = std::lower_bound(cdf.begin(), cdf.end(), u);
+                if (it != cdf.end()) cnt = (int)(it - cdf.begin());
+            }
+            cnt = std::min(cnt, i);
+            ds.sample(g, 0, i, cnt, cols);
+            b.row_dominant(g, i, cols);
+        }
+        return b.finish(out);
+    });
 }
 
 // Block-diagonal with dense lower-triangular blocks of size `block`.
 int sptrsv_gen_blockdiag(int n, int block, uint64_t seed, sptrsv_host_csr_t* out)
 {
-    if (!out || n < 0 || block < 1) return SPTRSV_ERR_INVALID_ARG;
-    memset(out, 0, sizeof(*out));
-    Rng g(seed);
-    Builder b;
-    std::vector<int> cols;
-    for (int i = 0; i < n; i++) {
-        cols.clear();
-        for (int c = (i / block) * block; c < i; c++) cols.push_back(c);
-        b.row_dominant(g, i, cols);
-    }
-    return b.finish(out);
+    return host_guard([&]() -> int {
+        if (!out || n < 0 || block < 1) return SPTRSV_ERR_INVALID_ARG;
+        memset(out, 0, sizeof(*out));
+        Rng g(seed);
+        Builder b;
+        std::vector<int> cols;
+        for (int i = 0; i < n; i++) {
+            cols.clear();
+            for (int c = (i / block) * block; c < i; c++) cols.push_back(c);
+            b.row_dominant(g, i, cols);
+        }
+        return b.finish(out);
+    });
 }
 
 void sptrsv_host_csr_free(sptrsv_host_csr_t* m)

@@ -5,7 +5,11 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <exception>
 #include <mutex>
+#include <new>
+#include <stdexcept>
+#include <system_error>
 #include <unordered_map>
 
 #include "common.cuh"
@@ -23,6 +27,38 @@ int cuda_fail(cudaError_t e, const char* where);
         cudaError_t e_ = (call);                                              \
         if (e_ != cudaSuccess) return ::sptrsv::cuda_fail(e_, #call);         \
     } while (0)
+
+// Every entry point of the C ABI runs its body through one of these, so no
+// C++ exception crosses the ABI: host memory, sizes or threads that cannot be
+// had (std::bad_alloc, std::length_error, std::system_error) become
+// SPTRSV_ERR_ALLOC, anything else SPTRSV_ERR_INVALID_ARG, with the message in
+// the thread's last error.  The void entry points (the reference's solver
+// and run_solver signatures) report through the last error only.
+template <class F>
+int abi_guard(F&& f) noexcept
+{
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return set_error(SPTRSV_ERR_ALLOC, "out of host memory");
+    } catch (const std::length_error& e) {
+        return set_error(SPTRSV_ERR_ALLOC, "host allocation too large: %s", e.what());
+    } catch (const std::system_error& e) {
+        return set_error(SPTRSV_ERR_ALLOC, "host resources: %s", e.what());
+    } catch (const std::exception& e) {
+        return set_error(SPTRSV_ERR_INVALID_ARG, "%s", e.what());
+    } catch (...) {
+        return set_error(SPTRSV_ERR_INVALID_ARG, "unknown exception");
+    }
+}
+template <class F>
+void abi_guard_void(F&& f) noexcept
+{
+    abi_guard([&]() -> int {
+        f();
+        return 0;
+    });
+}
 
 // ---- per-device context -------------------------------------------------
 struct Ctx {

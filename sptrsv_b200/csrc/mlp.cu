@@ -225,113 +225,129 @@ extern "C" {
 
 int sptrsv_mlp_create(uint64_t seed, sptrsv_mlp_t* out)
 {
-    if (!out) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_create: NULL");
-    if (!ctx()) return set_error(SPTRSV_ERR_CUDA, "mlp_create: no CUDA device");
-    sptrsv_mlp_s* M = new sptrsv_mlp_s();
-    auto fail = [&](int code) {
-        cudaFree(M->p); cudaFree(M->g); cudaFree(M->m); cudaFree(M->v); cudaFree(M->mean); cudaFree(M->sd);
-        delete M;
-        return code;
-    };
-    if (dalloc(&M->p, NPARAM) || dalloc(&M->g, NPARAM) || dalloc(&M->m, NPARAM) || dalloc(&M->v, NPARAM) ||
-        dalloc(&M->mean, NI) || dalloc(&M->sd, NI))
-        return fail(set_error(SPTRSV_ERR_ALLOC, "mlp_create: allocation failed"));
-    // He-uniform weights, zero biases
-    std::vector<float> h(NPARAM, 0.f);
-    std::mt19937_64 g(seed);
-    auto init = [&](int off, int fan_in, int count) {
-        float a = std::sqrt(6.f / (float)fan_in);
-        std::uniform_real_distribution<float> u(-a, a);
-        for (int i = 0; i < count; i++) h[off + i] = u(g);
-    };
-    init(O_W1, NI, NI * NH);
-    init(O_W2, NH, NH * NH);
-    init(O_W3, NH, NH * NO);
-    std::vector<float> mean(NI, 0.f), sd(NI, 1.f);
-    if (cudaMemcpy(M->p, h.data(), sizeof(float) * NPARAM, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(M->m, 0, sizeof(float) * NPARAM) != cudaSuccess ||
-        cudaMemset(M->v, 0, sizeof(float) * NPARAM) != cudaSuccess ||
-        cudaMemcpy(M->mean, mean.data(), sizeof(float) * NI, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(M->sd, sd.data(), sizeof(float) * NI, cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail(set_error(SPTRSV_ERR_CUDA, "mlp_create: upload failed"));
-    *out = M;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!out) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_create: NULL");
+        if (!ctx()) return set_error(SPTRSV_ERR_CUDA, "mlp_create: no CUDA device");
+        sptrsv_mlp_s* M = new sptrsv_mlp_s();
+        auto fail = [&](int code) {
+            cudaFree(M->p); cudaFree(M->g); cudaFree(M->m); cudaFree(M->v); cudaFree(M->mean); cudaFree(M->sd);
+            delete M;
+            return code;
+        };
+        if (dalloc(&M->p, NPARAM) || dalloc(&M->g, NPARAM) || dalloc(&M->m, NPARAM) || dalloc(&M->v, NPARAM) ||
+            dalloc(&M->mean, NI) || dalloc(&M->sd, NI))
+            return fail(set_error(SPTRSV_ERR_ALLOC, "mlp_create: allocation failed"));
+        // He-uniform weights, zero biases
+        std::vector<float> h(NPARAM, 0.f);
+        std::mt19937_64 g(seed);
+        auto init = [&](int off, int fan_in, int count) {
+            float a = std::sqrt(6.f / (float)fan_in);
+            std::uniform_real_distribution<float> u(-a, a);
+            for (int i = 0; i < count; i++) h[off + i] = u(g);
+        };
+        init(O_W1, NI, NI * NH);
+        init(O_W2, NH, NH * NH);
+        init(O_W3, NH, NH * NO);
+        std::vector<float> mean(NI, 0.f), sd(NI, 1.f);
+        if (cudaMemcpy(M->p, h.data(), sizeof(float) * NPARAM, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(M->m, 0, sizeof(float) * NPARAM) != cudaSuccess ||
+            cudaMemset(M->v, 0, sizeof(float) * NPARAM) != cudaSuccess ||
+            cudaMemcpy(M->mean, mean.data(), sizeof(float) * NI, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(M->sd, sd.data(), sizeof(float) * NI, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_error(SPTRSV_ERR_CUDA, "mlp_create: upload failed"));
+        *out = M;
+        return ok();
+    });
 }
 
 int sptrsv_mlp_destroy(sptrsv_mlp_t M)
 {
-    if (!M) return ok();
-    M->w.release();
-    cudaFree(M->p); cudaFree(M->g); cudaFree(M->m); cudaFree(M->v); cudaFree(M->mean); cudaFree(M->sd);
-    delete M;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M) return ok();
+        M->w.release();
+        cudaFree(M->p); cudaFree(M->g); cudaFree(M->m); cudaFree(M->v); cudaFree(M->mean); cudaFree(M->sd);
+        delete M;
+        return ok();
+    });
 }
 
 int sptrsv_mlp_get_params(sptrsv_mlp_t M, float* host)
 {
-    if (!M || !host) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_get_params: NULL");
-    SPT_CUDA(cudaMemcpy(host, M->p, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !host) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_get_params: NULL");
+        SPT_CUDA(cudaMemcpy(host, M->p, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
+        return ok();
+    });
 }
 
 int sptrsv_mlp_set_params(sptrsv_mlp_t M, const float* host)
 {
-    if (!M || !host) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_params: NULL");
-    SPT_CUDA(cudaMemcpy(M->p, host, sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
-    SPT_CUDA(cudaMemset(M->m, 0, sizeof(float) * NPARAM));
-    SPT_CUDA(cudaMemset(M->v, 0, sizeof(float) * NPARAM));
-    M->step = 0;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !host) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_params: NULL");
+        SPT_CUDA(cudaMemcpy(M->p, host, sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
+        SPT_CUDA(cudaMemset(M->m, 0, sizeof(float) * NPARAM));
+        SPT_CUDA(cudaMemset(M->v, 0, sizeof(float) * NPARAM));
+        M->step = 0;
+        return ok();
+    });
 }
 
 int sptrsv_mlp_set_normalization(sptrsv_mlp_t M, const float* mean12, const float* std12)
 {
-    if (!M || !mean12 || !std12) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_normalization: NULL");
-    for (int i = 0; i < NI; i++)
-        if (!(std12[i] > 0.f)) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_normalization: std must be > 0");
-    SPT_CUDA(cudaMemcpy(M->mean, mean12, sizeof(float) * NI, cudaMemcpyHostToDevice));
-    SPT_CUDA(cudaMemcpy(M->sd, std12, sizeof(float) * NI, cudaMemcpyHostToDevice));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !mean12 || !std12) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_normalization: NULL");
+        for (int i = 0; i < NI; i++)
+            if (!(std12[i] > 0.f)) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_set_normalization: std must be > 0");
+        SPT_CUDA(cudaMemcpy(M->mean, mean12, sizeof(float) * NI, cudaMemcpyHostToDevice));
+        SPT_CUDA(cudaMemcpy(M->sd, std12, sizeof(float) * NI, cudaMemcpyHostToDevice));
+        return ok();
+    });
 }
 
 int sptrsv_mlp_get_normalization(sptrsv_mlp_t M, float* mean12, float* std12)
 {
-    if (!M || !mean12 || !std12) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_get_normalization: NULL");
-    SPT_CUDA(cudaMemcpy(mean12, M->mean, sizeof(float) * NI, cudaMemcpyDeviceToHost));
-    SPT_CUDA(cudaMemcpy(std12, M->sd, sizeof(float) * NI, cudaMemcpyDeviceToHost));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !mean12 || !std12) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_get_normalization: NULL");
+        SPT_CUDA(cudaMemcpy(mean12, M->mean, sizeof(float) * NI, cudaMemcpyDeviceToHost));
+        SPT_CUDA(cudaMemcpy(std12, M->sd, sizeof(float) * NI, cudaMemcpyDeviceToHost));
+        return ok();
+    });
 }
 
 int sptrsv_mlp_forward_host(sptrsv_mlp_t M, const float* X, int B, float* Y)
 {
-    if (!M || !X || !Y || B < 1) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_forward: bad arguments");
-    int e = M->w.ensure(B);
-    if (e) return e;
-    SPT_CUDA(cudaMemcpy(M->w.bx, X, sizeof(float) * (size_t)B * NI, cudaMemcpyHostToDevice));
-    k_normalise<<<g1((long long)B * NI), 256>>>(M->w.bx, M->mean, M->sd, B, M->w.xn);
-    forward(M, B);
-    SPT_CUDA(cudaGetLastError());
-    SPT_CUDA(cudaMemcpy(Y, M->w.y, sizeof(float) * (size_t)B * NO, cudaMemcpyDeviceToHost));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !X || !Y || B < 1) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_forward: bad arguments");
+        int e = M->w.ensure(B);
+        if (e) return e;
+        SPT_CUDA(cudaMemcpy(M->w.bx, X, sizeof(float) * (size_t)B * NI, cudaMemcpyHostToDevice));
+        k_normalise<<<g1((long long)B * NI), 256>>>(M->w.bx, M->mean, M->sd, B, M->w.xn);
+        forward(M, B);
+        SPT_CUDA(cudaGetLastError());
+        SPT_CUDA(cudaMemcpy(Y, M->w.y, sizeof(float) * (size_t)B * NO, cudaMemcpyDeviceToHost));
+        return ok();
+    });
 }
 
 int sptrsv_mlp_gradient_host(sptrsv_mlp_t M, const float* X, const float* T, const float* Mk, int B, float* grad,
                              float* loss)
 {
-    if (!M || !X || !T || !Mk || B < 1) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_gradient: bad arguments");
-    int e = M->w.ensure(B);
-    if (e) return e;
-    MlpWork& w = M->w;
-    SPT_CUDA(cudaMemcpy(w.bx, X, sizeof(float) * (size_t)B * NI, cudaMemcpyHostToDevice));
-    SPT_CUDA(cudaMemcpy(w.bt, T, sizeof(float) * (size_t)B * NO, cudaMemcpyHostToDevice));
-    SPT_CUDA(cudaMemcpy(w.bm, Mk, sizeof(float) * (size_t)B * NO, cudaMemcpyHostToDevice));
-    k_normalise<<<g1((long long)B * NI), 256>>>(w.bx, M->mean, M->sd, B, w.xn);
-    forward(M, B);
-    backward(M, B, w.bt, w.bm, 1.f / mask_denom(Mk, (long long)B * NO));
-    SPT_CUDA(cudaGetLastError());
-    if (grad) SPT_CUDA(cudaMemcpy(grad, M->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
-    if (loss) SPT_CUDA(cudaMemcpy(loss, w.loss, sizeof(float), cudaMemcpyDeviceToHost));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !X || !T || !Mk || B < 1) return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_gradient: bad arguments");
+        int e = M->w.ensure(B);
+        if (e) return e;
+        MlpWork& w = M->w;
+        SPT_CUDA(cudaMemcpy(w.bx, X, sizeof(float) * (size_t)B * NI, cudaMemcpyHostToDevice));
+        SPT_CUDA(cudaMemcpy(w.bt, T, sizeof(float) * (size_t)B * NO, cudaMemcpyHostToDevice));
+        SPT_CUDA(cudaMemcpy(w.bm, Mk, sizeof(float) * (size_t)B * NO, cudaMemcpyHostToDevice));
+        k_normalise<<<g1((long long)B * NI), 256>>>(w.bx, M->mean, M->sd, B, w.xn);
+        forward(M, B);
+        backward(M, B, w.bt, w.bm, 1.f / mask_denom(Mk, (long long)B * NO));
+        SPT_CUDA(cudaGetLastError());
+        if (grad) SPT_CUDA(cudaMemcpy(grad, M->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
+        if (loss) SPT_CUDA(cudaMemcpy(loss, w.loss, sizeof(float), cudaMemcpyDeviceToHost));
+        return ok();
+    });
 }
 
 // Minibatch Adam over a dataset of N rows held on the device for the call.
@@ -339,56 +355,58 @@ int sptrsv_mlp_gradient_host(sptrsv_mlp_t M, const float* X, const float* T, con
 int sptrsv_mlp_train_host(sptrsv_mlp_t M, const float* X, const float* T, const float* Mk, int N, int epochs,
                           int batch, float lr, uint64_t seed, float* loss_curve)
 {
-    if (!M || !X || !T || !Mk || N < 1 || epochs < 0 || batch < 1 || !(lr > 0.f))
-        return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_train: bad arguments");
-    if (batch > N) batch = N;
-    int e = M->w.ensure(batch);
-    if (e) return e;
-    float *dX = nullptr, *dT = nullptr, *dM = nullptr;
-    auto cleanup = [&]() { cudaFree(dX); cudaFree(dT); cudaFree(dM); };
-    if (dalloc(&dX, (long long)N * NI) || dalloc(&dT, (long long)N * NO) || dalloc(&dM, (long long)N * NO)) {
-        cleanup();
-        return set_error(SPTRSV_ERR_ALLOC, "mlp_train: allocation failed");
-    }
-    cudaMemcpy(dX, X, sizeof(float) * (size_t)N * NI, cudaMemcpyHostToDevice);
-    cudaMemcpy(dT, T, sizeof(float) * (size_t)N * NO, cudaMemcpyHostToDevice);
-    cudaMemcpy(dM, Mk, sizeof(float) * (size_t)N * NO, cudaMemcpyHostToDevice);
-    std::mt19937_64 g(seed);
-    std::vector<int> perm(N);
-    for (int i = 0; i < N; i++) perm[i] = i;
-    MlpWork& w = M->w;
-    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    std::vector<float> mh((size_t)batch * NO);
-    for (int ep = 0; ep < epochs; ep++) {
-        std::shuffle(perm.begin(), perm.end(), g);
-        double lsum = 0;
-        int nb = 0;
-        for (int s = 0; s < N; s += batch) {
-            int B = std::min(batch, N - s);
-            cudaMemcpy(w.idx, perm.data() + s, sizeof(int) * B, cudaMemcpyHostToDevice);
-            k_gather_rows<<<g1((long long)B * NI), 256>>>(dX, w.idx, B, NI, w.bx);
-            k_gather_rows<<<g1((long long)B * NO), 256>>>(dT, w.idx, B, NO, w.bt);
-            k_gather_rows<<<g1((long long)B * NO), 256>>>(dM, w.idx, B, NO, w.bm);
-            double msum = 0;
-            for (int b = 0; b < B; b++)
-                for (int c = 0; c < NO; c++) msum += Mk[(size_t)perm[s + b] * NO + c];
-            k_normalise<<<g1((long long)B * NI), 256>>>(w.bx, M->mean, M->sd, B, w.xn);
-            forward(M, B);
-            backward(M, B, w.bt, w.bm, 1.f / (float)(msum > 1 ? msum : 1));
-            M->step++;
-            float c1 = 1.f - std::pow(b1, (float)M->step), c2 = 1.f - std::pow(b2, (float)M->step);
-            k_adam<<<g1(NPARAM), 256>>>(M->p, M->g, M->m, M->v, NPARAM, lr, b1, b2, eps, c1, c2);
-            float lh = 0;
-            cudaMemcpy(&lh, w.loss, sizeof(float), cudaMemcpyDeviceToHost);
-            lsum += lh;
-            nb++;
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!M || !X || !T || !Mk || N < 1 || epochs < 0 || batch < 1 || !(lr > 0.f))
+            return set_error(SPTRSV_ERR_INVALID_ARG, "mlp_train: bad arguments");
+        if (batch > N) batch = N;
+        int e = M->w.ensure(batch);
+        if (e) return e;
+        float *dX = nullptr, *dT = nullptr, *dM = nullptr;
+        auto cleanup = [&]() { cudaFree(dX); cudaFree(dT); cudaFree(dM); };
+        if (dalloc(&dX, (long long)N * NI) || dalloc(&dT, (long long)N * NO) || dalloc(&dM, (long long)N * NO)) {
+            cleanup();
+            return set_error(SPTRSV_ERR_ALLOC, "mlp_train: allocation failed");
         }
-        if (loss_curve) loss_curve[ep] = (float)(lsum / (nb ? nb : 1));
-    }
-    cleanup();
-    cudaError_t ce = cudaGetLastError();
-    if (ce != cudaSuccess) return cuda_fail(ce, "mlp_train");
-    return ok();
+        cudaMemcpy(dX, X, sizeof(float) * (size_t)N * NI, cudaMemcpyHostToDevice);
+        cudaMemcpy(dT, T, sizeof(float) * (size_t)N * NO, cudaMemcpyHostToDevice);
+        cudaMemcpy(dM, Mk, sizeof(float) * (size_t)N * NO, cudaMemcpyHostToDevice);
+        std::mt19937_64 g(seed);
+        std::vector<int> perm(N);
+        for (int i = 0; i < N; i++) perm[i] = i;
+        MlpWork& w = M->w;
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        std::vector<float> mh((size_t)batch * NO);
+        for (int ep = 0; ep < epochs; ep++) {
+            std::shuffle(perm.begin(), perm.end(), g);
+            double lsum = 0;
+            int nb = 0;
+            for (int s = 0; s < N; s += batch) {
+                int B = std::min(batch, N - s);
+                cudaMemcpy(w.idx, perm.data() + s, sizeof(int) * B, cudaMemcpyHostToDevice);
+                k_gather_rows<<<g1((long long)B * NI), 256>>>(dX, w.idx, B, NI, w.bx);
+                k_gather_rows<<<g1((long long)B * NO), 256>>>(dT, w.idx, B, NO, w.bt);
+                k_gather_rows<<<g1((long long)B * NO), 256>>>(dM, w.idx, B, NO, w.bm);
+                double msum = 0;
+                for (int b = 0; b < B; b++)
+                    for (int c = 0; c < NO; c++) msum += Mk[(size_t)perm[s + b] * NO + c];
+                k_normalise<<<g1((long long)B * NI), 256>>>(w.bx, M->mean, M->sd, B, w.xn);
+                forward(M, B);
+                backward(M, B, w.bt, w.bm, 1.f / (float)(msum > 1 ? msum : 1));
+                M->step++;
+                float c1 = 1.f - std::pow(b1, (float)M->step), c2 = 1.f - std::pow(b2, (float)M->step);
+                k_adam<<<g1(NPARAM), 256>>>(M->p, M->g, M->m, M->v, NPARAM, lr, b1, b2, eps, c1, c2);
+                float lh = 0;
+                cudaMemcpy(&lh, w.loss, sizeof(float), cudaMemcpyDeviceToHost);
+                lsum += lh;
+                nb++;
+            }
+            if (loss_curve) loss_curve[ep] = (float)(lsum / (nb ? nb : 1));
+        }
+        cleanup();
+        cudaError_t ce = cudaGetLastError();
+        if (ce != cudaSuccess) return cuda_fail(ce, "mlp_train");
+        return ok();
+    });
 }
 
 }  // extern "C"

@@ -122,43 +122,45 @@ using namespace sptrsv;
 extern "C" int sptrsv_solve_ir_noalloc(const sp_mat_t* L, const double* b, double* x, int ir_iters,
                                        cudaStream_t stream)
 {
-    if (!L || !b || !x || ir_iters < 0 || ir_iters > 16 || L->nr < 0 || L->nc != L->nr || L->nnz < L->nr ||
-        (L->nr > 0 && (!L->ia || !L->ja || !L->a)))
-        return set_error(SPTRSV_ERR_INVALID_ARG, "solve_ir_noalloc: bad arguments");
-    if ((long long)L->nr > kNoallocMaxRows)
-        return set_error(SPTRSV_ERR_UNSUPPORTED,
-                         "solve_ir_noalloc: n = %d exceeds the fixed scratch limit of %lld rows", L->nr,
-                         kNoallocMaxRows);
-    const int n = L->nr;
-    if (n == 0) return ok();
-    unsigned char* base = nullptr;
-    int sms = 0;
-    int e = scratch_address(&base, &sms);
-    if (e) return e;
-    float* x32 = reinterpret_cast<float*>(base);
-    float* r32 = x32 + kNoallocMaxRows;
-    DevStatus* st = reinterpret_cast<DevStatus*>(base + 2 * sizeof(float) * kNoallocMaxRows);
-    // the array keeps the previous call's contents: reset what must start clean
-    SPT_CUDA(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream));
-    SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)n, stream));
-    NatMat m{L->ia, L->ja, L->a, nullptr, L->nnz};
-    SPT_CUDA((launch_chunk<double, OUT_SET64>(m, n, b, x32, x, st, sms, stream)));
-    long long rgrid = ((long long)n * 32 + 255) / 256;  // one warp per row, at most 16 blocks per SM
-    if (rgrid > 16LL * sms) rgrid = 16LL * sms;
-    for (int it = 0; it < ir_iters; it++) {
-        k_residual_nat<<<(int)rgrid, 256, 0, stream>>>(L->ia, L->ja, L->a, n, L->nnz, b, x, r32, st);
-        SPT_CUDA(cudaGetLastError());
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!L || !b || !x || ir_iters < 0 || ir_iters > 16 || L->nr < 0 || L->nc != L->nr || L->nnz < L->nr ||
+            (L->nr > 0 && (!L->ia || !L->ja || !L->a)))
+            return set_error(SPTRSV_ERR_INVALID_ARG, "solve_ir_noalloc: bad arguments");
+        if ((long long)L->nr > kNoallocMaxRows)
+            return set_error(SPTRSV_ERR_UNSUPPORTED,
+                             "solve_ir_noalloc: n = %d exceeds the fixed scratch limit of %lld rows", L->nr,
+                             kNoallocMaxRows);
+        const int n = L->nr;
+        if (n == 0) return ok();
+        unsigned char* base = nullptr;
+        int sms = 0;
+        int e = scratch_address(&base, &sms);
+        if (e) return e;
+        float* x32 = reinterpret_cast<float*>(base);
+        float* r32 = x32 + kNoallocMaxRows;
+        DevStatus* st = reinterpret_cast<DevStatus*>(base + 2 * sizeof(float) * kNoallocMaxRows);
+        // the array keeps the previous call's contents: reset what must start clean
+        SPT_CUDA(cudaMemsetAsync(st, 0, sizeof(DevStatus), stream));
         SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)n, stream));
-        SPT_CUDA((launch_chunk<float, OUT_ADD64>(m, n, r32, x32, x, st, sms, stream)));
-    }
-    DevStatus h{};
-    SPT_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
-    SPT_CUDA(cudaStreamSynchronize(stream));
-    if (h.code == SPTRSV_ERR_INVALID_CSR)
-        return set_error(SPTRSV_ERR_INVALID_CSR,
-                         "solve_ir_noalloc: row %d is not lower-triangular CSR with the diagonal last", h.row);
-    if (h.code == SPTRSV_ERR_TIMEOUT)
-        return set_error(SPTRSV_ERR_TIMEOUT, "solve_ir_noalloc: device wait ran out of budget at row %d", h.row);
-    if (h.code != 0) return set_error(h.code, "solve_ir_noalloc: device error %d at row %d", h.code, h.row);
-    return ok();
+        NatMat m{L->ia, L->ja, L->a, nullptr, L->nnz};
+        SPT_CUDA((launch_chunk<double, OUT_SET64>(m, n, b, x32, x, st, sms, stream)));
+        long long rgrid = ((long long)n * 32 + 255) / 256;  // one warp per row, at most 16 blocks per SM
+        if (rgrid > 16LL * sms) rgrid = 16LL * sms;
+        for (int it = 0; it < ir_iters; it++) {
+            k_residual_nat<<<(int)rgrid, 256, 0, stream>>>(L->ia, L->ja, L->a, n, L->nnz, b, x, r32, st);
+            SPT_CUDA(cudaGetLastError());
+            SPT_CUDA(cudaMemsetAsync(x32, 0xFF, sizeof(float) * (size_t)n, stream));
+            SPT_CUDA((launch_chunk<float, OUT_ADD64>(m, n, r32, x32, x, st, sms, stream)));
+        }
+        DevStatus h{};
+        SPT_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
+        SPT_CUDA(cudaStreamSynchronize(stream));
+        if (h.code == SPTRSV_ERR_INVALID_CSR)
+            return set_error(SPTRSV_ERR_INVALID_CSR,
+                             "solve_ir_noalloc: row %d is not lower-triangular CSR with the diagonal last", h.row);
+        if (h.code == SPTRSV_ERR_TIMEOUT)
+            return set_error(SPTRSV_ERR_TIMEOUT, "solve_ir_noalloc: device wait ran out of budget at row %d", h.row);
+        if (h.code != 0) return set_error(h.code, "solve_ir_noalloc: device error %d at row %d", h.code, h.row);
+        return ok();
+    });
 }

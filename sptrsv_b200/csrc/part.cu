@@ -550,41 +550,45 @@ using namespace sptrsv;
 // partitions = P.
 extern "C" int sptrsv_partition_blocks_host(const struct sptrsv_host_csr_s* m, int P, int* table, double* bound)
 {
-    if (!m || !table || m->n < 1 || !m->rowptr || !m->colidx || !m->val)
-        return set_error(SPTRSV_ERR_INVALID_ARG, "partition_blocks_host: bad arguments");
-    if ((long long)m->n < 256LL * P)
-        return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: %d rows are too few for %d blocks of >= 256 rows", m->n,
-                         P);
-    int bad = -1;
-    int e = sptrsv_check_csr_host(m->rowptr, m->colidx, m->n, &bad);
-    if (e) return e;
-    std::vector<int> tab;
-    int w = 0;
-    double b = 0;
-    e = partition_blocks(m->rowptr, m->colidx, m->val, m->n, P, (int)std::thread::hardware_concurrency(), tab, &w,
-                         &b, 0.0);
-    if (e) return e;
-    long long next = 0;
-    for (int i = 0; i < P; i++) {
-        tab[4 * i + 3] = (int)next;
-        next += tab[4 * i + 2] - tab[4 * i];
-    }
-    std::copy(tab.begin(), tab.end(), table);
-    if (bound) *bound = b;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!m || !table || m->n < 1 || !m->rowptr || !m->colidx || !m->val)
+            return set_error(SPTRSV_ERR_INVALID_ARG, "partition_blocks_host: bad arguments");
+        if ((long long)m->n < 256LL * P)
+            return set_error(SPTRSV_ERR_UNSUPPORTED, "partitions: %d rows are too few for %d blocks of >= 256 rows", m->n,
+                             P);
+        int bad = -1;
+        int e = sptrsv_check_csr_host(m->rowptr, m->colidx, m->n, &bad);
+        if (e) return e;
+        std::vector<int> tab;
+        int w = 0;
+        double b = 0;
+        e = partition_blocks(m->rowptr, m->colidx, m->val, m->n, P, (int)std::thread::hardware_concurrency(), tab, &w,
+                             &b, 0.0);
+        if (e) return e;
+        long long next = 0;
+        for (int i = 0; i < P; i++) {
+            tab[4 * i + 3] = (int)next;
+            next += tab[4 * i + 2] - tab[4 * i];
+        }
+        std::copy(tab.begin(), tab.end(), table);
+        if (bound) *bound = b;
+        return ok();
+    });
 }
 
 extern "C" int sptrsv_plan_partition_info(sptrsv_plan_t p, int* blocks, int* n_ext, long long* warm_rows,
                                           double* bound, int* table)
 {
-    if (!p) return set_error(SPTRSV_ERR_INVALID_ARG, "partition_info: NULL plan");
-    if (!p->part || p->sched.partitions < 2)
-        return set_error(SPTRSV_ERR_INVALID_ARG, "partition_info: the plan's schedule is not partitioned");
-    const PartPlan* q = p->part;
-    if (blocks) *blocks = q->P;
-    if (n_ext) *n_ext = q->n_ext;
-    if (warm_rows) *warm_rows = q->warm_rows;
-    if (bound) *bound = q->bound;
-    if (table) std::copy(q->tab.begin(), q->tab.end(), table);
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p) return set_error(SPTRSV_ERR_INVALID_ARG, "partition_info: NULL plan");
+        if (!p->part || p->sched.partitions < 2)
+            return set_error(SPTRSV_ERR_INVALID_ARG, "partition_info: the plan's schedule is not partitioned");
+        const PartPlan* q = p->part;
+        if (blocks) *blocks = q->P;
+        if (n_ext) *n_ext = q->n_ext;
+        if (warm_rows) *warm_rows = q->warm_rows;
+        if (bound) *bound = q->bound;
+        if (table) std::copy(q->tab.begin(), q->tab.end(), table);
+        return ok();
+    });
 }

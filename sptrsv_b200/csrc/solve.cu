@@ -704,249 +704,281 @@ extern "C" {
 
 void csr_L_solve_simple(sp_mat_t* mat, const VALUE_TYPE* b, VALUE_TYPE* x, int n, int* is_solved)
 {
-    (void)is_solved;
-    solve_reference(mat, nullptr, b, x, n, SIMPLE, 0, 0);
+    ::sptrsv::abi_guard_void([&] {
+        (void)is_solved;
+        solve_reference(mat, nullptr, b, x, n, SIMPLE, 0, 0);
+    });
 }
 
 void csr_L_solve_order(sp_mat_t* mat, dfr_analysis_info_t* info, const VALUE_TYPE* b, VALUE_TYPE* x, int n,
                        cudaStream_t stream)
 {
-    solve_reference(mat, info, b, x, n, ORDER, 32, stream);
+    ::sptrsv::abi_guard_void([&] {
+        solve_reference(mat, info, b, x, n, ORDER, 32, stream);
+    });
 }
 
 void csr_L_solve_multirow(sp_mat_t* mat, dfr_analysis_info_t* info, const VALUE_TYPE* b, VALUE_TYPE* x, int n,
                           cudaStream_t stream)
 {
-    solve_reference(mat, info, b, x, n, MULTIROW, 0, stream);
+    ::sptrsv::abi_guard_void([&] {
+        solve_reference(mat, info, b, x, n, MULTIROW, 0, stream);
+    });
 }
 
 int sptrsv_solve_order_tile(sp_mat_t* mat, dfr_analysis_info_t* info, const double* b, double* x, int tile,
                             cudaStream_t stream)
 {
-    if (!pow2_lanes(tile)) return set_error(SPTRSV_ERR_INVALID_ARG, "order_tile: tile must be 1,2,4,8,16,32");
-    return solve_reference(mat, info, b, x, mat ? mat->nr : -1, ORDER, tile, stream);
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!pow2_lanes(tile)) return set_error(SPTRSV_ERR_INVALID_ARG, "order_tile: tile must be 1,2,4,8,16,32");
+        return solve_reference(mat, info, b, x, mat ? mat->nr : -1, ORDER, tile, stream);
+    });
 }
 
 int sptrsv_plan_create(const sp_mat_t* L, const dfr_analysis_info_t* info, sptrsv_plan_t* out)
 {
-    if (!L || !info || !out) return set_error(SPTRSV_ERR_INVALID_ARG, "plan_create: NULL argument");
-    *out = nullptr;
-    AnalysisRec* rec = find_analysis(info->row_ctr);
-    if (!rec || !info->iorder || rec->n != L->nr)
-        return set_error(SPTRSV_ERR_NOT_ANALYSED, "plan_create: info is not an analysis of this matrix");
-    Ctx* c = ctx();
-    if (!c) return set_error(SPTRSV_ERR_CUDA, "plan_create: no CUDA device");
-    cudaStream_t s = 0;
-    sptrsv_plan_s* p = new sptrsv_plan_s();
-    p->device = c->device;
-    p->n = L->nr;
-    p->nnz_off = L->nnz - L->nr;
-    p->nlevs = rec->nlevs;
-    p->n_warps = rec->n_warps;
-    p->sched = default_schedule();
-    const int n = p->n;
-    int* d_scr = nullptr;
-    auto fail = [&](int code) {
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!L || !info || !out) return set_error(SPTRSV_ERR_INVALID_ARG, "plan_create: NULL argument");
+        *out = nullptr;
+        AnalysisRec* rec = find_analysis(info->row_ctr);
+        if (!rec || !info->iorder || rec->n != L->nr)
+            return set_error(SPTRSV_ERR_NOT_ANALYSED, "plan_create: info is not an analysis of this matrix");
+        Ctx* c = ctx();
+        if (!c) return set_error(SPTRSV_ERR_CUDA, "plan_create: no CUDA device");
+        cudaStream_t s = 0;
+        sptrsv_plan_s* p = new sptrsv_plan_s();
+        p->device = c->device;
+        p->n = L->nr;
+        p->nnz_off = L->nnz - L->nr;
+        p->nlevs = rec->nlevs;
+        p->n_warps = rec->n_warps;
+        p->sched = default_schedule();
+        const int n = p->n;
+        int* d_scr = nullptr;
+        auto fail = [&](int code) {
+            cudaFree(d_scr);
+            plan_free_arrays(p);
+            delete p;
+            return code;
+        };
+    #define PCHK(call)                                                \
+        do {                                                          \
+            cudaError_t e_ = (call);                                  \
+            if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
+        } while (0)
+        {
+            int e = layout_alloc(p->lev, n, p->nnz_off);
+            if (e) return fail(e);
+        }
+        PCHK(dalloc(&p->inv, n));
+        PCHK(dalloc(&p->levels, n));
+        PCHK(dalloc(&p->ibase, (long long)p->n_warps + 1));
+        PCHK(dalloc(&p->ivect, p->n_warps));
+        PCHK(dalloc(&d_scr, scan_scratch_ints((long long)n + 1)));
+        if (n > 0) {
+            k_plan_rows<<<grid_for((long long)n + 1, 256), 256, 0, s>>>(L->ia, info->iorder, n, p->lev.ptr, p->lev.rowid);
+            PCHK(cudaGetLastError());
+            PCHK(scan_exclusive(p->lev.ptr, p->lev.ptr, (long long)n + 1, d_scr, s));
+            int e = plan_fill_values(p, L, s);
+            if (e) return fail(e);
+            PCHK(cudaMemcpyAsync(p->inv, info->inv_iorder, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+            PCHK(cudaMemcpyAsync(p->levels, rec->d_levels, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        }
+        PCHK(cudaMemcpyAsync(p->ibase, rec->d_ibase, sizeof(int) * ((size_t)p->n_warps + 1), cudaMemcpyDeviceToDevice, s));
+        if (p->n_warps > 0)
+            PCHK(cudaMemcpyAsync(p->ivect, rec->d_ivect, sizeof(int) * (size_t)p->n_warps, cudaMemcpyDeviceToDevice, s));
+        PCHK(cudaStreamSynchronize(s));
+    #undef PCHK
         cudaFree(d_scr);
-        plan_free_arrays(p);
-        delete p;
-        return code;
-    };
-#define PCHK(call)                                                \
-    do {                                                          \
-        cudaError_t e_ = (call);                                  \
-        if (e_ != cudaSuccess) return fail(cuda_fail(e_, #call)); \
-    } while (0)
-    {
-        int e = layout_alloc(p->lev, n, p->nnz_off);
-        if (e) return fail(e);
-    }
-    PCHK(dalloc(&p->inv, n));
-    PCHK(dalloc(&p->levels, n));
-    PCHK(dalloc(&p->ibase, (long long)p->n_warps + 1));
-    PCHK(dalloc(&p->ivect, p->n_warps));
-    PCHK(dalloc(&d_scr, scan_scratch_ints((long long)n + 1)));
-    if (n > 0) {
-        k_plan_rows<<<grid_for((long long)n + 1, 256), 256, 0, s>>>(L->ia, info->iorder, n, p->lev.ptr, p->lev.rowid);
-        PCHK(cudaGetLastError());
-        PCHK(scan_exclusive(p->lev.ptr, p->lev.ptr, (long long)n + 1, d_scr, s));
-        int e = plan_fill_values(p, L, s);
-        if (e) return fail(e);
-        PCHK(cudaMemcpyAsync(p->inv, info->inv_iorder, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-        PCHK(cudaMemcpyAsync(p->levels, rec->d_levels, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    }
-    PCHK(cudaMemcpyAsync(p->ibase, rec->d_ibase, sizeof(int) * ((size_t)p->n_warps + 1), cudaMemcpyDeviceToDevice, s));
-    if (p->n_warps > 0)
-        PCHK(cudaMemcpyAsync(p->ivect, rec->d_ivect, sizeof(int) * (size_t)p->n_warps, cudaMemcpyDeviceToDevice, s));
-    PCHK(cudaStreamSynchronize(s));
-#undef PCHK
-    cudaFree(d_scr);
-    *out = p;
-    return ok();
+        *out = p;
+        return ok();
+    });
 }
 
 int sptrsv_plan_destroy(sptrsv_plan_t p)
 {
-    if (!p) return ok();
-    plan_free_arrays(p);
-    delete p;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p) return ok();
+        plan_free_arrays(p);
+        delete p;
+        return ok();
+    });
 }
 
 int sptrsv_plan_set_schedule(sptrsv_plan_t p, const sptrsv_schedule_t* s)
 {
-    if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: NULL argument");
-    int e = check_schedule(s);
-    if (e) return e;
-    if (s->partitions >= 2) {
-        // the variant runs on the block system; if it cannot, the plan keeps
-        // the block system its current schedule uses
-        PartPlan* prev = p->part;
-        e = build_part(p, s->partitions);
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "set_schedule: NULL argument");
+        int e = check_schedule(s);
         if (e) return e;
-        sptrsv_schedule_t inner = *s;
-        inner.partitions = 0;
-        e = sptrsv_plan_set_schedule(p->part->sub, &inner);
-        if (e) {
-            if (p->part != prev && p->part_alt == prev) std::swap(p->part, p->part_alt);
-            return e;
+        if (s->partitions >= 2) {
+            // the variant runs on the block system; if it cannot, the plan keeps
+            // the block system its current schedule uses
+            PartPlan* prev = p->part;
+            e = build_part(p, s->partitions);
+            if (e) return e;
+            sptrsv_schedule_t inner = *s;
+            inner.partitions = 0;
+            e = sptrsv_plan_set_schedule(p->part->sub, &inner);
+            if (e) {
+                if (p->part != prev && p->part_alt == prev) std::swap(p->part, p->part_alt);
+                return e;
+            }
+        } else if (s->variant == SPTRSV_VAR_CLUSTER) {
+            e = build_cluster_layout(p, s->band_levels, s->cluster_rows);
+            if (!e) e = build_cluster_tasks(p, s->rows_per_warp);
+            if (e) return e;
+        } else if (s->variant == SPTRSV_VAR_ORDER) {
+            e = build_order_tasks(p, s->rows_per_warp);
+            if (e) return e;
+        } else if (s->variant == SPTRSV_VAR_STRIP) {
+            e = build_strip_layout(p, s->rows_per_warp);
+            if (e) return e;
+        } else if (s->variant == SPTRSV_VAR_WAVE) {
+            e = build_wave_layout(p, s->block_warps, kWaveMaxRows);
+            if (e) return e;
+        } else if (s->variant == SPTRSV_VAR_BAND) {
+            e = build_band_layout(p);
+            if (e) return e;
         }
-    } else if (s->variant == SPTRSV_VAR_CLUSTER) {
-        e = build_cluster_layout(p, s->band_levels, s->cluster_rows);
-        if (!e) e = build_cluster_tasks(p, s->rows_per_warp);
-        if (e) return e;
-    } else if (s->variant == SPTRSV_VAR_ORDER) {
-        e = build_order_tasks(p, s->rows_per_warp);
-        if (e) return e;
-    } else if (s->variant == SPTRSV_VAR_STRIP) {
-        e = build_strip_layout(p, s->rows_per_warp);
-        if (e) return e;
-    } else if (s->variant == SPTRSV_VAR_WAVE) {
-        e = build_wave_layout(p, s->block_warps, kWaveMaxRows);
-        if (e) return e;
-    } else if (s->variant == SPTRSV_VAR_BAND) {
-        e = build_band_layout(p);
-        if (e) return e;
-    }
-    p->sched = *s;
-    return ok();
+        p->sched = *s;
+        return ok();
+    });
 }
 
 int sptrsv_plan_set_stream_segment(sptrsv_plan_t p, int rows)
 {
-    if (!p || rows < 0 || rows % 16 != 0)
-        return set_error(SPTRSV_ERR_INVALID_ARG, "set_stream_segment: rows must be 0 or a positive multiple of 16");
-    p->seg_rows = rows;
-    cudaFree(p->bflag);  // the flag words are sized by the segment count
-    p->bflag = nullptr;
-    p->nseg = 0;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || rows < 0 || rows % 16 != 0)
+            return set_error(SPTRSV_ERR_INVALID_ARG, "set_stream_segment: rows must be 0 or a positive multiple of 16");
+        p->seg_rows = rows;
+        cudaFree(p->bflag);  // the flag words are sized by the segment count
+        p->bflag = nullptr;
+        p->nseg = 0;
+        return ok();
+    });
 }
 
 int sptrsv_plan_get_schedule(sptrsv_plan_t p, sptrsv_schedule_t* s)
 {
-    if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "get_schedule: NULL argument");
-    *s = p->sched;
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !s) return set_error(SPTRSV_ERR_INVALID_ARG, "get_schedule: NULL argument");
+        *s = p->sched;
+        return ok();
+    });
 }
 
 int sptrsv_plan_update_values(sptrsv_plan_t p, const sp_mat_t* L)
 {
-    if (!p || !L || L->nr != p->n || L->nnz - L->nr != p->nnz_off)
-        return set_error(SPTRSV_ERR_INVALID_ARG, "update_values: matrix does not match the plan");
-    int e = plan_fill_values(p, L, 0);
-    if (e) return e;
-    SPT_CUDA(cudaStreamSynchronize(0));
-    return ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !L || L->nr != p->n || L->nnz - L->nr != p->nnz_off)
+            return set_error(SPTRSV_ERR_INVALID_ARG, "update_values: matrix does not match the plan");
+        int e = plan_fill_values(p, L, 0);
+        if (e) return e;
+        SPT_CUDA(cudaStreamSynchronize(0));
+        return ok();
+    });
 }
 
 int sptrsv_solve_f64(sptrsv_plan_t p, const double* b, double* x, int nrhs, cudaStream_t stream)
 {
-    if (!p || !b || !x || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f64: bad arguments");
-    if (p->n == 0) return ok();
-    int e = plan_solve_f64(p, b, x, nrhs, stream);
-    return e ? e : ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !b || !x || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f64: bad arguments");
+        if (p->n == 0) return ok();
+        int e = plan_solve_f64(p, b, x, nrhs, stream);
+        return e ? e : ok();
+    });
 }
 
 int sptrsv_solve_ir(sptrsv_plan_t p, const double* b, double* x, int nrhs, cudaStream_t stream)
 {
-    if (!p || !b || !x || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_ir: bad arguments");
-    if (p->n == 0) return ok();
-    int e = plan_solve_ir(p, b, x, nrhs, stream);
-    return e ? e : ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !b || !x || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_ir: bad arguments");
+        if (p->n == 0) return ok();
+        int e = plan_solve_ir(p, b, x, nrhs, stream);
+        return e ? e : ok();
+    });
 }
 
 int sptrsv_solve_f32(sptrsv_plan_t p, const double* b, float* x32, int nrhs, cudaStream_t stream)
 {
-    if (!p || !b || !x32 || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f32: bad arguments");
-    if (p->n == 0) return ok();
-    int e = solve32<double>(p, b, x32, nullptr, OUT_X, nrhs, stream);
-    return e ? e : ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !b || !x32 || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "solve_f32: bad arguments");
+        if (p->n == 0) return ok();
+        int e = solve32<double>(p, b, x32, nullptr, OUT_X, nrhs, stream);
+        return e ? e : ok();
+    });
 }
 
 int sptrsv_plan_calibrate_ir(sptrsv_plan_t p, const double* b, double* x, int nrhs, double tol, int max_iters,
                              int* iters, double* est)
 {
-    if (!p || !b || !x || nrhs < 1 || nrhs > 32 || !(tol > 0) || max_iters < 0 || max_iters > 16)
-        return set_error(SPTRSV_ERR_INVALID_ARG, "calibrate_ir: bad arguments");
-    if (p->n == 0) {
-        if (iters) *iters = 0;
-        return ok();
-    }
-    int need = max_iters;
-    double r = 0;
-    int e = plan_calibrate_ir(p, b, x, nrhs, tol, max_iters, &need, &r);
-    if (e) return e;
-    if (r > tol && need >= max_iters) {
-        p->sched.ir_max_iters = max_iters;
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !b || !x || nrhs < 1 || nrhs > 32 || !(tol > 0) || max_iters < 0 || max_iters > 16)
+            return set_error(SPTRSV_ERR_INVALID_ARG, "calibrate_ir: bad arguments");
+        if (p->n == 0) {
+            if (iters) *iters = 0;
+            return ok();
+        }
+        int need = max_iters;
+        double r = 0;
+        int e = plan_calibrate_ir(p, b, x, nrhs, tol, max_iters, &need, &r);
+        if (e) return e;
+        if (r > tol && need >= max_iters) {
+            p->sched.ir_max_iters = max_iters;
+            if (iters) *iters = need;
+            if (est) *est = r;
+            return set_error(SPTRSV_ERR_NOT_CONVERGED, "calibrate_ir: correction/x = %.3g after %d steps", r, max_iters);
+        }
+        p->sched.ir_max_iters = need;
         if (iters) *iters = need;
         if (est) *est = r;
-        return set_error(SPTRSV_ERR_NOT_CONVERGED, "calibrate_ir: correction/x = %.3g after %d steps", r, max_iters);
-    }
-    p->sched.ir_max_iters = need;
-    if (iters) *iters = need;
-    if (est) *est = r;
-    return ok();
+        return ok();
+    });
 }
 
 int sptrsv_residual_f64(sptrsv_plan_t p, const double* b, const double* x, double* r, int nrhs, cudaStream_t stream)
 {
-    if (!p || !b || !x || !r || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "residual: bad arguments");
-    if (p->n == 0) return ok();
-    int e = plan_residual(p, b, x, nullptr, r, nrhs, stream);
-    return e ? e : ok();
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !b || !x || !r || nrhs < 1 || nrhs > 32) return set_error(SPTRSV_ERR_INVALID_ARG, "residual: bad arguments");
+        if (p->n == 0) return ok();
+        int e = plan_residual(p, b, x, nullptr, r, nrhs, stream);
+        return e ? e : ok();
+    });
 }
 
 int sptrsv_solve_host(sptrsv_plan_t p, const double* hb, double* hx, int nrhs, int precision, cudaStream_t s)
 {
-    if (!p || !hb || !hx || nrhs < 1 || nrhs > 32 || (precision != 32 && precision != 64))
-        return set_error(SPTRSV_ERR_INVALID_ARG, "solve_host: bad arguments");
-    if (p->n == 0) return ok();
-    const size_t bytes = sizeof(double) * (size_t)p->n * nrhs;
-    if (nrhs > p->cap_host) {
-        cudaFree(p->hb);
-        cudaFree(p->hx);
-        p->hb = p->hx = nullptr;
-        p->cap_host = 0;
-        SPT_CUDA(cudaMalloc((void**)&p->hb, bytes));
-        SPT_CUDA(cudaMalloc((void**)&p->hx, bytes));
-        p->cap_host = nrhs;
-    }
-    void* hx_dev = nullptr;
-    if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && mapped_host(hb) &&
-        (hx_dev = mapped_host(hx)) != nullptr) {
-        int e = partitioned(p) ? 0 : build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
-        if (!e) e = solve_host_streamed(p, hb, (double*)hx_dev, s);
+    return ::sptrsv::abi_guard([&]() -> int {
+        if (!p || !hb || !hx || nrhs < 1 || nrhs > 32 || (precision != 32 && precision != 64))
+            return set_error(SPTRSV_ERR_INVALID_ARG, "solve_host: bad arguments");
+        if (p->n == 0) return ok();
+        const size_t bytes = sizeof(double) * (size_t)p->n * nrhs;
+        if (nrhs > p->cap_host) {
+            cudaFree(p->hb);
+            cudaFree(p->hx);
+            p->hb = p->hx = nullptr;
+            p->cap_host = 0;
+            SPT_CUDA(cudaMalloc((void**)&p->hb, bytes));
+            SPT_CUDA(cudaMalloc((void**)&p->hx, bytes));
+            p->cap_host = nrhs;
+        }
+        void* hx_dev = nullptr;
+        if (nrhs == 1 && precision == 64 && p->sched.variant == SPTRSV_VAR_WAVE && mapped_host(hb) &&
+            (hx_dev = mapped_host(hx)) != nullptr) {
+            int e = partitioned(p) ? 0 : build_wave_layout(p, p->sched.block_warps, kWaveMaxRows);
+            if (!e) e = solve_host_streamed(p, hb, (double*)hx_dev, s);
+            if (e) return e;
+            e = sync_status(s);
+            return e ? e : ok();
+        }
+        SPT_CUDA(cudaMemcpyAsync(p->hb, hb, bytes, cudaMemcpyHostToDevice, s));
+        int e = precision == 32 ? plan_solve_ir(p, p->hb, p->hx, nrhs, s) : plan_solve_f64(p, p->hb, p->hx, nrhs, s);
         if (e) return e;
+        SPT_CUDA(cudaMemcpyAsync(hx, p->hx, bytes, cudaMemcpyDeviceToHost, s));
         e = sync_status(s);
         return e ? e : ok();
-    }
-    SPT_CUDA(cudaMemcpyAsync(p->hb, hb, bytes, cudaMemcpyHostToDevice, s));
-    int e = precision == 32 ? plan_solve_ir(p, p->hb, p->hx, nrhs, s) : plan_solve_f64(p, p->hb, p->hx, nrhs, s);
-    if (e) return e;
-    SPT_CUDA(cudaMemcpyAsync(hx, p->hx, bytes, cudaMemcpyDeviceToHost, s));
-    e = sync_status(s);
-    return e ? e : ok();
+    });
 }
 
 }  // extern "C"
