@@ -20,9 +20,11 @@
  * success and a negative SPTRSV_ERR_* code on failure (the reference only
  * printed, header/common.h:163-168).  Functions that return void in the
  * reference record their outcome in a thread-local last error, read with
- * sptrsv_last_error() / sptrsv_last_error_string().  No device wait in this
- * library is unbounded: a wait that runs out sets a device status word and
- * returns, and the host reports SPTRSV_ERR_TIMEOUT.
+ * sptrsv_last_error() / sptrsv_last_error_string().  No C++ exception
+ * leaves the library: host memory, sizes or threads that cannot be had give
+ * SPTRSV_ERR_ALLOC.  No device wait in this library is unbounded: a wait
+ * that runs out sets a device status word and returns, and the host reports
+ * SPTRSV_ERR_TIMEOUT.
  */
 #ifndef SPTRSV_B200_H
 #define SPTRSV_B200_H
