@@ -195,3 +195,32 @@ def test_null_handles_and_arguments_are_refused_without_a_crash():
             assert code == -6, (name, code)  # SPTRSV_ERR_NOT_ANALYSED
         else:
             assert code == -2, (name, code)  # SPTRSV_ERR_INVALID_ARG
+
+
+def test_integration_examples_compile_and_link(tmp_path):
+    """The C examples of the integration guide's C section, in order, compile
+    as C99 against the header and link against the library (they are not
+    run: they need a GPU)."""
+    import subprocess
+
+    text = (ROOT / "INTEGRATION.md").read_text()
+    text = text[:text.index("## 2.")]  # section 1, the C callers (later sections are other languages' stubs)
+    blocks = re.findall(r"```c\n(.*?)```", text, flags=re.S)
+    assert len(blocks) >= 5
+    body = []
+    for blk in blocks:
+        # the batch example's nrhs is the per-system array, elsewhere a count
+        body.append("{ const int* nrhs = 0;\n" + blk + "}\n" if "sptrsv_batch_create" in blk else blk)
+    src = tmp_path / "examples.c"
+    src.write_text('#include "sptrsv_b200.h"\n'
+                   "int main(void) {\n"
+                   "int* rowptr = 0; int* colidx = 0; double* val = 0; int n = 0; double* b = 0; double* x = 0;\n"
+                   "double* d_b = 0; double* d_x = 0; int nrhs = 1; cudaStream_t stream = 0;\n"
+                   "sptrsv_host_csr_t host_csr = {0}; int nsys = 0; sp_mat_t* mats = 0;\n"
+                   + "\n".join(body) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "examples"
+    lib = ROOT / "sptrsv_b200"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-Wno-unused-variable", "-Wno-unused-but-set-variable",
+                        "-Wno-maybe-uninitialized", "-Wno-uninitialized", f"-I{ROOT / 'include'}", str(src), f"-L{lib}",
+                        "-lsptrsv_b200", "-Wl,--allow-shlib-undefined", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
