@@ -30,3 +30,25 @@ def test_selector_reproduces_reported_regret():
     # the learned choice beats the reference's own rule (its multirow solver) on held-out matrices
     ref = T[:, ev["reference_rule"]["class"]]
     assert float(np.exp(np.mean(np.log(ref / chosen)))) > 1.1
+
+
+def test_targets_and_evaluation_on_a_small_table():
+    """The training targets (log2 of time over the best, masked where a class
+    did not run) and the evaluation's regret, top-1 and geometric mean, on a
+    table small enough to check by hand."""
+    from sptrsv_b200 import select as SEL
+    from sptrsv_b200 import train_selector as TS
+
+    t = np.full((2, SEL.N_CLASSES), np.nan, dtype=np.float32)
+    t[0, :3] = [2.0, 1.0, 4.0]
+    t[1, 5], t[1, 7] = 3.0, 6.0
+    T, M = SEL.targets_from_times(t)
+    assert np.array_equal(M[0, :4], [1, 1, 1, 0]) and M[1].sum() == 2
+    assert np.allclose(T[0, :3], [1.0, 0.0, 2.0]) and np.allclose(T[1, [5, 7]], [0.0, 1.0])
+    assert np.all(T[M == 0] == 0)
+    ev = TS.evaluate(t, np.array([0, 5]))  # 2x the best on the first matrix, the best on the second
+    assert np.isclose(ev["mean_regret"], 0.5) and np.isclose(ev["top1"], 0.5)
+    assert np.isclose(ev["geomean_time_over_best"], np.sqrt(2.0))
+    # a choice that did not run counts as the slowest class that did
+    ev = TS.evaluate(t, np.array([1, 0]))
+    assert np.isclose(ev["mean_regret"], 0.5) and np.isclose(ev["top1"], 0.5)
