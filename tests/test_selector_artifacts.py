@@ -52,3 +52,20 @@ def test_targets_and_evaluation_on_a_small_table():
     # a choice that did not run counts as the slowest class that did
     ev = TS.evaluate(t, np.array([1, 0]))
     assert np.isclose(ev["mean_regret"], 0.5) and np.isclose(ev["top1"], 0.5)
+
+
+def test_class_table_names_and_the_reference_rule():
+    """The 24 schedule classes have distinct names; the indexes the stored
+    selector data and the evaluation rely on are fixed: class 12 is the
+    reference's own rule (its multirow solver, 8-warp blocks, no back-off),
+    class 4 WAVE over 16 blocks, class 23 BAND over 128 blocks."""
+    from sptrsv_b200 import select as SEL
+
+    names = [SEL.class_name(c) for c in range(SEL.N_CLASSES)]
+    assert len(set(names)) == SEL.N_CLASSES
+    assert names[12] == "multirow/bw8-bo0-wps0" and names[4] == "wave/G4-P16" and names[23] == "band-P128"
+    ev = json.loads((PKG / "selector_eval.json").read_text()) if (PKG / "selector_eval.json").exists() else None
+    if ev is not None:
+        assert ev["reference_rule"]["class"] == 12 and ev["reference_rule"]["name"] == names[12]
+    with pytest.raises(Exception):
+        SEL.schedule_from_class(SEL.N_CLASSES)
