@@ -262,7 +262,8 @@ def host_flush(buf):
 
 
 def run_reference(args, rank, world, dist):
-    """The reference's algorithm on the host cores (CPU oracle, all threads).
+    """The reference's algorithm on the host cores (CPU oracle): the faster of
+    its level-scheduled form on all threads and its serial form on one core.
     Inputs come from the oracle's own copy of the generators, so this arm
     neither imports nor loads the product library."""
     if rank != 0:
@@ -279,20 +280,36 @@ def run_reference(args, rank, world, dist):
     a = O.analysis(m.rowptr, m.colidx)
     lev_ptr = np.concatenate([[0], np.cumsum(np.bincount(a["levels"] - 1, minlength=a["nlevs"]))]).astype(np.int32)
     threads = O.num_threads()
-    x = O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
+    # two CPU forms of the reference's substitution: level-scheduled on every host thread (a barrier per
+    # level) and serial on one core; the arm times the faster of the two on this workload
+    forms = {
+        "level": (lambda: O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k),
+                  threads, f"level-scheduled on {threads} threads, {a['nlevs']} levels"),
+        "serial": (lambda: O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k), 1, "serial substitution on one core"),
+    }
+    probe_ms = {}
+    for name, (fn, _, _) in forms.items():
+        fn()
+        t0 = time.perf_counter()
+        fn()
+        probe_ms[name] = 1e3 * (time.perf_counter() - t0)
+    pick = min(probe_ms, key=probe_ms.get)
+    solve_fn, threads, how = forms[pick]
+    x = solve_fn()
     err = O.rel_err(x, O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k))
     flush_buf = np.empty(256 << 20, dtype=np.uint8)
     for _ in range(args.warmup):
-        O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
+        solve_fn()
     times = []
     for _ in range(args.steps):
         host_flush(flush_buf)
         t0 = time.perf_counter()
-        O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lev_ptr, a["nlevs"], k)
+        solve_fn()
         times.append(time.perf_counter() - t0)
     total = sum(times)
     v = k * args.steps / total
-    sample = f"{args.steps} full solves of {args.config} (level-scheduled, {a['nlevs']} levels)"
+    sample = (f"{args.steps} full solves of {args.config} ({how}; the faster CPU form in a probe: "
+              + ", ".join(f"{f} {t:.2f} ms" for f, t in probe_ms.items()) + ")")
     line = {
         "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
@@ -300,39 +317,42 @@ def run_reference(args, rank, world, dist):
         "config": workload_config(args.config, m.n, m.nnz, a["nlevs"], k, world),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "gb_s": algorithmic_bytes(m.n, m.nnz, k) * v / 1e9, "rel_err_vs_serial": err,
+        "gb_s": algorithmic_bytes(m.n, m.nnz, k) * v / 1e9, "rel_err_vs_serial": err, "cpu_form": pick,
+        "probe_ms": probe_ms,
     }
     print(json.dumps(line), flush=True)
     barrier(dist)
 
 
 def run_reference_batch(args, world, dist):
-    """Batched configuration on the host cores: each system's level-scheduled
-    FP64 substitution on all threads, systems one after another; a step is a
-    bounded sample (systems in order until about 2 s), value = RHS solved / s."""
+    """Batched configuration on the host cores: the systems are independent,
+    so every host thread takes whole systems, each by the serial FP64
+    substitution; a step is a bounded sample (the systems in order, a few per
+    thread at a time, until about 2 s), value = RHS solved / s."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from oracle import oracle as O
     from oracle import workloads as W
 
     mats, ks, xs = W.batch_config(512, seed=3)
     threads = O.num_threads()
-    prep = []
-    for m, x, k in zip(mats, xs, ks):
-        a = O.analysis(m.rowptr, m.colidx)
-        lev_ptr = np.concatenate([[0], np.cumsum(np.bincount(a["levels"] - 1, minlength=a["nlevs"]))]).astype(np.int32)
-        prep.append((m, m.matvec(x, k), k, a, lev_ptr))
+    prep = [(m, m.matvec(x, k), k) for m, x, k in zip(mats, xs, ks)]
     flush_buf = np.empty(256 << 20, dtype=np.uint8)
+    pool = ThreadPoolExecutor(max_workers=threads)  # the oracle's C calls release the GIL
+
+    def solve_one(item):
+        m, b, k = item
+        O.solve(m.rowptr, m.colidx, m.val, b, nrhs=k)
+        return k
 
     def step():
-        done, t = 0, 0.0
         host_flush(flush_buf)
-        for m, b, k, a, lp in prep:
-            t0 = time.perf_counter()
-            O.solve_levels_omp(m.rowptr, m.colidx, m.val, b, a["iorder"], lp, a["nlevs"], k)
-            t += time.perf_counter() - t0
-            done += k
-            if t > 2.0:
-                break
-        return done, t
+        done, t0, i = 0, time.perf_counter(), 0
+        while i < len(prep) and time.perf_counter() - t0 < 2.0:
+            chunk = prep[i:i + 4 * threads]
+            done += sum(pool.map(solve_one, chunk))
+            i += len(chunk)
+        return done, time.perf_counter() - t0
 
     for _ in range(args.warmup):
         step()
@@ -341,8 +361,10 @@ def run_reference_batch(args, world, dist):
         d, t = step()
         done += d
         total += t
+    pool.shutdown()
     v = done / total
-    sample = f"{args.steps} steps, each the first systems of the batch in order until 2 s (level-scheduled)"
+    sample = (f"{args.steps} steps, each the systems of the batch in order until 2 s, {threads} threads taking "
+              "whole systems (serial substitution each)")
     line = {
         "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
