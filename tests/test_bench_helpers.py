@@ -60,3 +60,37 @@ def test_traffic_of_every_bench_schedule_is_on_record():
     for key in ("wave_p16_f64_c1", "band_p128_f64_c0", "multirow_f64_c2k16", "batch_p4096_f64_c3"):
         t = bench.load_traffic(key)
         assert isinstance(t, int) and t > 0, key
+
+
+_REF_ARM = r"""
+import json, runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--config", "c0", "--steps", "2", "--warmup", "3"]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit as e:
+    assert not e.code, e.code
+maps = open("/proc/self/maps").read()
+print(json.dumps({"mapped": "libsptrsv_b200" in maps, "imported": any(m.startswith("sptrsv_b200") for m in sys.modules)}))
+"""
+
+
+def test_reference_arm_line_and_isolation():
+    """The reference arm (CPU, the small banded configuration) prints one line
+    with the contract's keys, picks the faster CPU form, and neither imports
+    nor maps the product library."""
+    import json
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    r = subprocess.run([sys.executable, "-c", _REF_ARM], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines() if x.startswith("{")]
+    line, iso = lines[-2], lines[-1]
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "solves/s"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["cpu_form"] in ("level", "serial") and line["rel_err_vs_serial"] <= 1e-12
+    assert line["probe_ms"][line["cpu_form"]] == min(line["probe_ms"].values())
+    assert set(line["config"]) >= {"workload", "n", "nnz", "nlevs", "nrhs"}
+    assert iso == {"mapped": False, "imported": False}
